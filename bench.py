@@ -1,0 +1,309 @@
+"""Benchmark of the B200 SIPG solve path.
+
+Workload (the metric's configuration): SIPG Helmholtz (alpha = k^2 = 5) on a
+256 x 256 quad grid of [0,1]^2 split into 131072 triangles, N = 4 (Np = 15,
+1,966,080 DOFs), Dirichlet on x = 0, 1 and Neumann on y = 0, 1, penalty
+tau = (N+1)^2 / h (tau_scale = 0.5), RHS = sum of 8 seeded Fourier modes
+(integer wavenumbers 1..6, N(0,1) amplitudes, seed 0).
+
+One step = one float64 operator apply (y = (alpha M + A) u) over the whole
+mesh, inputs resident in HBM; L2 is flushed (256 MB write) between timed
+steps and only the apply itself is timed (CUDA events on the launching
+stream).  value = DOFs / apply time (GDOF/s).  The JSON line also reports
+the float32 apply, the mixed-precision vs float64 block-Jacobi PCG solves
+(solves/s, latency, relative error), the roofline of the dominant kernel,
+the end-to-end rate through the public API with host buffers, and the CPU
+baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SIPG matvec GDOF/s; solves/s + p99 latency at 1e-8 err, mixed vs FP64 on GPU"
+KX = KY = 256
+NDEG = 4
+ALPHA = 5.0
+TAU_SCALE = 0.5
+
+
+def workload_arrays(build_mesh, uniform_mesh):
+    VX, VY, E = uniform_mesh(0.0, 1.0, 0.0, 1.0, KX, KY)
+    m = build_mesh(VX, VY, E, NDEG)
+    isb = m.EToE == np.arange(m.K)[:, None]
+    nxf = m.nx.reshape((m.Nfp, 3, m.K), order="F")[0].T
+    bc = np.where(isb, np.where(np.abs(nxf) > 0.5, 1, 2), 0).astype(np.int32)
+    rng = np.random.default_rng(0)
+    kx = rng.integers(1, 7, size=8)
+    ky = rng.integers(1, 7, size=8)
+    amp = rng.standard_normal(8)
+    f = sum(a * np.sin(np.pi * i * m.x) * np.cos(np.pi * j * m.y) for a, i, j in zip(amp, kx, ky))
+    return m, bc, f
+
+
+def algorithmic_bytes(K, Np, sv, sg):
+    """B_apply = K [2 Np s_v + 14 s_g + 12]: u read, y written, 14 geometry
+    scalars per element, 3 packed int32 neighbour words."""
+    return K * (2 * Np * sv + 14 * sg + 12)
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, dev):
+        self.dev, self.samples, self.proc = dev, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 9
+                          for i in range(4) if s[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    m, bc, f = workload_arrays(pm.build_mesh_2d, pm.uniform_rectangle_mesh_2d)
+    op = m.device_operator(bc, TAU_SCALE)
+    n = op.n
+    g = torch.Generator(device=dev).manual_seed(1 + rank)
+    u64 = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    y64 = torch.empty_like(u64)
+    u32 = u64.float()
+    y32 = torch.empty_like(u32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def timed_applies(u, y, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            op.apply(u, alpha=ALPHA, out=y)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) * 1e-3 for a, b in ev]
+
+    for _ in range(args.warmup):
+        op.apply(u64, alpha=ALPHA, out=y64)
+        op.apply(u32, alpha=ALPHA, out=y32)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        t64 = timed_applies(u64, y64, args.steps)
+        t32 = timed_applies(u32, y32, args.steps)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    tot64 = sum(t64)
+    if world > 1:
+        tt = torch.tensor([tot64], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot64 = float(tt.item())
+    ms_step = tot64 / args.steps * 1e3
+    value = world * n * args.steps / tot64 / 1e9
+    a64 = float(np.mean(t64))
+    a32 = float(np.mean(t32))
+    hbm, peak_kind = peaks()
+    B64 = algorithmic_bytes(m.K, m.Np, 8, 8)
+    B32 = algorithmic_bytes(m.K, m.Np, 4, 4)
+
+    # ---- end to end through the public API: host numpy in, host numpy out
+    u_host = np.random.default_rng(2).standard_normal((m.Np, m.K))
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        ps.sipg_apply_2d(m, u_host, bc_types=bc, tau_scale=TAU_SCALE)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        yh = ps.sipg_apply_2d(m, u_host, bc_types=bc, tau_scale=TAU_SCALE)
+    torch.cuda.synchronize()
+    te2e = (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": world * n / te2e / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": int(u_host.nbytes),
+           "d2h_bytes_per_step": int(yh.nbytes), "note": "sipg_apply_2d(numpy) incl. H2D/D2H; alpha=0"}
+
+    # ---- solves: float64 PCG vs mixed-precision refinement (rel err 1e-8 target)
+    solves = None
+    if not args.skip_solves:
+        pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=ALPHA, nu=1.0, bc_types=bc,
+                                                           tau_scale=TAU_SCALE)
+        ref_u = ps.solve_sipg_helmholtz_2d(m, f, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE,
+                                           preconditioner=pc,
+                                           iterative=ps.IterativeConfig(tol=1e-13, maxiter=20000))
+        out = {}
+        for name, cfg in (("fp64", ps.IterativeConfig(tol=args.solve_tol, maxiter=20000)),
+                          ("mixed", ps.IterativeConfig(tol=args.solve_tol, maxiter=20000, precision="mixed",
+                                                       inner_tol=args.inner_tol))):
+            lat, info, u = [], None, None
+            for _ in range(args.solve_reps + 1):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                u, info = ps.solve_sipg_helmholtz_2d(m, f, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE,
+                                                     preconditioner=pc, iterative=cfg, return_info=True)
+                lat.append(time.perf_counter() - t0)
+            lat = lat[1:]
+            out[name] = {"solves_per_s": 1.0 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                         "p99_ms": float(np.percentile(lat, 99) * 1e3), "iterations": info.iterations,
+                         "refinements": info.refinements, "status": info.status,
+                         "rel_err_vs_fp64_tol1e-13": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u))}
+        out["speedup_mixed_vs_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+        out["note"] = ("block-Jacobi PCG, tol %.0e; latency = host wall clock of the public API call "
+                       "(numpy in/out); reference solution = float64 device PCG at tol 1e-13" % args.solve_tol)
+        solves = out
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "precision: Helmholtz k^2=5, 256x256 quads -> 131072 triangles, N=4, "
+                               "1,966,080 DOFs, Dirichlet x / Neumann y, tau_scale=0.5",
+                   "step": "one float64 operator apply (alpha M + A) u",
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": "replicas"},
+        "apply_fp32": {"gdofs": n / a32 / 1e9, "us": a32 * 1e6},
+        "roofline": {"bound": "hbm", "achieved": B64 / a64 / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": B64 / a64 / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "k_apply<4,double,APPLY>", "algorithmic_bytes": B64},
+        "roofline_fp32": {"bound": "hbm", "achieved": B32 / a32 / 1e9, "peak": hbm, "unit": "GB/s",
+                          "frac": B32 / a32 / 1e9 / hbm, "kernel": "k_apply<4,float,APPLY>",
+                          "algorithmic_bytes": B32},
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "solves": solves,
+    }
+    if rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_baseline(budget_s=args.cpu_seconds)
+    return line
+
+
+# ------------------------------------------------------------ CPU legs
+
+def cpu_baseline(budget_s=15.0):
+    """The oracle's float64 apply on the host cores, bounded sample."""
+    from oracle import cbuild
+    return cbuild.time_apply(KX, KY, NDEG, TAU_SCALE, ALPHA, budget_s=budget_s)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import cbuild
+    res = []
+    for _ in range(args.warmup):
+        cbuild.time_apply(KX, KY, NDEG, TAU_SCALE, ALPHA, budget_s=1.0, reps=1)
+    for _ in range(args.steps):
+        res.append(cbuild.time_apply(KX, KY, NDEG, TAU_SCALE, ALPHA, budget_s=1.0, reps=1))
+    v = float(np.median([r["value"] for r in res]))
+    cb = dict(res[-1])
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": "GDOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * (KX * KY * 2 * 15) / (v * 1e9),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": "precision: Helmholtz k^2=5, 256x256 quads -> 131072 triangles, N=4, "
+                                   "1,966,080 DOFs, Dirichlet x / Neumann y, tau_scale=0.5",
+                       "step": "one float64 operator apply on the host cores"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solve-tol", type=float, default=1e-12)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--solve-reps", type=int, default=3)
+    ap.add_argument("--skip-solves", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,421 @@
+// Device code of the matrix-free SIPG operator (sm_100a).
+//
+// One thread owns one element.  The reference-element matrices (Dr, Ds, M,
+// the three face masses) live in __constant__ memory per degree and
+// precision; every thread of a warp reads the same entry at the same time,
+// so each multiply-add takes its matrix operand straight from the constant
+// bank.  Element tiles of the element-major vectors are staged into shared
+// memory with TMA bulk copies (cp.async.bulk) and written back the same way.
+//
+// The operator is the gradient of ddg's SIPG bilinear form
+// (src/ddg/dg2d/sipg.py:142-337) written "gather-only": every element
+// computes all contributions to its own nodes, including the ones the
+// reference scatters from the neighbouring element's side of a shared face,
+// so no atomics are needed.  For an interior face (own side M, neighbour P,
+// w = 1/2 from each side, sipg.py:135-138):
+//   y[Fmask_f]  += sJ * m1d_f^T ( -c_a * avg + c_j * jmp )
+//   g_x[Fmask_f] -= sJ * nx * m1d_f^T ( c_g * jmp )      (g_y likewise)
+//   y           += Dr^T (rx gx + ry gy) + Ds^T (sx gx + sy gy),
+//   gx = M^T (J ux) + face part,
+// with avg = (Dn_M + Dn_P)/2, jmp = u_M - u_P and the coefficients
+//   own side:  interior c_a=1/2, c_j=tau_M/2, c_g=1/4;
+//              Dirichlet c_a=1, c_j=tau_M, c_g=1 (avg=Dn_M, jmp=u_M);
+//   neighbour side (its tag interior): c_a+=1/2, c_j+=tau_P/2, c_g+=1/4,
+// tau = tau_scale (N+1)^2 sJ / J on each side (sipg.py:263).
+//
+// The neighbour's normal derivative at the shared face needs face rows of
+// Dr/Ds for the neighbour's face f'.  To keep the constant-bank operands
+// uniform across a warp (f' differs between neighbouring threads), the
+// neighbour's nodal values are gathered through a rotation permutation that
+// relabels its vertices so that f' becomes face 0; the chain-rule
+// coefficients are rotated to match.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ddg {
+
+template <int N>
+struct Dim {
+  static constexpr int Np = (N + 1) * (N + 2) / 2;
+  static constexpr int Nfp = N + 1;
+};
+
+// Face-node indices of the row-by-row warp-and-blend numbering.
+__host__ __device__ constexpr int fmask_idx(int N, int f, int p) {
+  return f == 0 ? p : (f == 1 ? p * (N + 1) - p * (p - 1) / 2 + (N - p) : p * (N + 1) - p * (p - 1) / 2);
+}
+
+template <int N, typename T>
+struct RefMats {
+  T Dr[Dim<N>::Np * Dim<N>::Np];
+  T Ds[Dim<N>::Np * Dim<N>::Np];
+  T M[Dim<N>::Np * Dim<N>::Np];
+  T m1d[3 * Dim<N>::Nfp * Dim<N>::Nfp];
+};
+
+// Constant-memory matrices are defined in sipg_kernels.cu, which also
+// specialises CRef for every built degree.
+template <int N, typename T> struct CRef;
+
+// ---------------------------------------------------------------- layout
+// Geometry: structure-of-arrays geo[c * ldg + k].
+enum GeoField { G_RX = 0, G_SX, G_RY, G_SY, G_J, G_F0 = 5, G_COUNT = 14 };
+// Neighbour word per (face f, element k), nbr[f * K + k]:
+//   bits 0-1 neighbour face f' | bit 2 flip | bits 3-4 BC tag of (k,f)
+//   bit 5 neighbour side contributes (its tag interior, real neighbour)
+//   bit 6 own side interior active (tag interior, real neighbour)
+//   bits 7-31 neighbour element k'
+__host__ __device__ constexpr uint32_t nbr_pack(uint32_t kp, uint32_t fp, bool flip, uint32_t bc,
+                                                bool pact, bool mint) {
+  return fp | (flip ? 4u : 0u) | (bc << 3) | (pact ? 32u : 0u) | (mint ? 64u : 0u) | (kp << 7);
+}
+constexpr uint32_t NBR_MAX_K = (1u << 25) - 1u;
+
+// Device status word bits (written by kernels, read by the host).
+enum DevStatus : unsigned int { ST_TMA_TIMEOUT = 1u, ST_BAD_INDEX = 2u };
+
+// ------------------------------------------------------- PTX helpers (TMA)
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(sdst)),
+      "l"(gsrc), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_addr(ssrc)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait on a bulk-copy barrier; on timeout records ST_TMA_TIMEOUT and
+// returns false (the caller then skips the tile; nothing spins forever).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, unsigned int* status) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, phase)) return true;
+  atomicOr(status, ST_TMA_TIMEOUT);
+  return false;
+}
+
+// ------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block sum of two doubles; the result is valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* s_red) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    s_red[warp] = a;
+    s_red[32 + warp] = b;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    a = lane < BLOCK / 32 ? s_red[lane] : 0.0;
+    b = lane < BLOCK / 32 ? s_red[32 + lane] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+  }
+}
+
+// "Last block done" detection (threadfence reduction).  Every block has
+// written its partials before calling; returns true in exactly one block.
+__device__ __forceinline__ bool is_last_block(unsigned int* ticket) {
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  return s_last;
+}
+
+// Deterministic sum of n partials (fixed order) by one block; valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ void reduce_partials2(const double* pa, const double* pb, int n, double& a, double& b,
+                                                 double* s_red) {
+  a = 0.0;
+  b = 0.0;
+  for (int i = threadIdx.x; i < n; i += BLOCK) {
+    a += __ldcg(pa + i);
+    if (pb) b += __ldcg(pb + i);
+  }
+  block_sum2<BLOCK>(a, b, s_red);
+}
+
+// --------------------------------------------------- CG control block
+struct CgCtl {
+  double gamma;   // r.z
+  double pAp;
+  double alpha;
+  double beta;
+  double rr;      // r.r
+  double bb;      // b.b
+  double atol2;   // max(tol^2 b.b, atol^2)
+  double tol2, atol_sq;
+  int iter, maxiter, status, use_pc;
+  int cont;       // loop condition mirror (1 = keep iterating)
+  unsigned int ticket;
+  unsigned int dev_status;
+  int pad;
+};
+
+// ---------------------------------------------------- element operator
+template <typename T>
+struct Geo {
+  T rx, sx, ry, sy, J;
+  T nx[3], ny[3], sJ[3];
+};
+
+template <typename T>
+__device__ __forceinline__ Geo<T> load_geo(const T* __restrict__ geo, int ldg, int k) {
+  Geo<T> g;
+  g.rx = __ldg(geo + G_RX * ldg + k);
+  g.sx = __ldg(geo + G_SX * ldg + k);
+  g.ry = __ldg(geo + G_RY * ldg + k);
+  g.sy = __ldg(geo + G_SY * ldg + k);
+  g.J = __ldg(geo + G_J * ldg + k);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    g.nx[f] = __ldg(geo + (G_F0 + 3 * f) * ldg + k);
+    g.ny[f] = __ldg(geo + (G_F0 + 3 * f + 1) * ldg + k);
+    g.sJ[f] = __ldg(geo + (G_F0 + 3 * f + 2) * ldg + k);
+  }
+  return g;
+}
+
+// Neighbour-value sources (the rotated neighbour vector u~ of face f').
+template <typename T, int Np>
+struct NbrPlain {  // u~[i] = u[k' Np + perm[f'][i]]
+  const T* __restrict__ u;
+  const int* perm;  // shared memory, 3*Np
+  __device__ __forceinline__ void operator()(int kp, int fp, T (&ut)[Np]) const {
+    const T* base = u + (size_t)kp * Np;
+#pragma unroll
+    for (int i = 0; i < Np; ++i) ut[i] = __ldg(base + perm[fp * Np + i]);
+  }
+};
+template <typename T, int Np>
+struct NbrPfuse {  // u~ = z~ + beta p_old~  (the CG direction update, fused)
+  const T* __restrict__ z;
+  const T* __restrict__ p;
+  T beta;
+  const int* perm;
+  __device__ __forceinline__ void operator()(int kp, int fp, T (&ut)[Np]) const {
+    const size_t o = (size_t)kp * Np;
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      const int j = perm[fp * Np + i];
+      ut[i] = __ldg(z + o + j) + beta * __ldg(p + o + j);
+    }
+  }
+};
+template <typename T, int Np>
+struct NbrZero {  // self-block extraction: the neighbour carries no value
+  __device__ __forceinline__ void operator()(int, int, T (&ut)[Np]) const {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) ut[i] = T(0);
+  }
+};
+
+// y = A u + alpha J M u  for element k (u, y in registers).
+// USE_NBR=false skips the neighbour value gather (self-block mode: the
+// neighbour's value is zero, its geometry still sets tau_P).
+template <int N, typename T, bool USE_NBR, class NbrSrc>
+__device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<N>::Np], const Geo<T>& g,
+                                           const uint32_t (&w)[3], const T* __restrict__ geo, int ldg, T tau,
+                                           T alpha, const NbrSrc& nbr) {
+  constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
+  const RefMats<N, T>& R = CRef<N, T>::get();
+
+  // physical gradient at the nodes
+  T ux[Np], uy[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    T ar = T(0), as = T(0);
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      ar = fma(R.Dr[i * Np + j], u[j], ar);
+      as = fma(R.Ds[i * Np + j], u[j], as);
+    }
+    ux[i] = g.rx * ar + g.sx * as;
+    uy[i] = g.ry * ar + g.sy * as;
+  }
+  // own normal derivative at face nodes
+  T dnm[3][Nfp];
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const int n = fmask_idx(N, f, p);
+      dnm[f][p] = g.nx[f] * ux[n] + g.ny[f] * uy[n];
+    }
+  // volume part of the lifted gradient: ex = M^T (J ux), ey = M^T (J uy)
+  T ex[Np], ey[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    T a = T(0), b = T(0);
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      a = fma(R.M[j * Np + i], ux[j], a);
+      b = fma(R.M[j * Np + i], uy[j], b);
+    }
+    ex[i] = g.J * a;
+    ey[i] = g.J * b;
+  }
+  // mass term (Helmholtz): alpha J (M u)
+#pragma unroll
+  for (int i = 0; i < Np; ++i) y[i] = T(0);
+  if (alpha != T(0)) {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      T a = T(0);
+#pragma unroll
+      for (int j = 0; j < Np; ++j) a = fma(R.M[i * Np + j], u[j], a);
+      y[i] = alpha * g.J * a;
+    }
+  }
+  // faces
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const uint32_t wf = w[f];
+    const int bc = (wf >> 3) & 3;
+    const bool pact = (wf >> 5) & 1;
+    const bool mint = (wf >> 6) & 1;
+    const bool mdir = (bc == 1);
+    if (!(pact || mint || mdir)) continue;
+    const T sJ = g.sJ[f], nx = g.nx[f], ny = g.ny[f];
+    const T tauM = tau * sJ / g.J;
+    T uP[Nfp], dnP[Nfp];
+    T tauP = tauM;
+    if (pact || mint) {
+      const int kp = (int)(wf >> 7), fp = (int)(wf & 3);
+      const bool flip = (wf >> 2) & 1;
+      const T rxn = __ldg(geo + G_RX * ldg + kp), sxn = __ldg(geo + G_SX * ldg + kp);
+      const T ryn = __ldg(geo + G_RY * ldg + kp), syn = __ldg(geo + G_SY * ldg + kp);
+      const T Jn = __ldg(geo + G_J * ldg + kp);
+      tauP = tau * sJ / Jn;
+      if (USE_NBR) {
+        T ut[Np];
+        nbr(kp, fp, ut);
+        const T ar = nx * rxn + ny * ryn, as = nx * sxn + ny * syn;
+        // derivative along the re-labelled reference axes (r~, s~)
+        const T cr = fp == 0 ? ar : (fp == 1 ? as : -ar - as);
+        const T cs = fp == 0 ? as : (fp == 1 ? -ar - as : ar);
+        T dq[Nfp];
+#pragma unroll
+        for (int q = 0; q < Nfp; ++q) {
+          T a = T(0), b = T(0);
+#pragma unroll
+          for (int j = 0; j < Np; ++j) {
+            a = fma(R.Dr[q * Np + j], ut[j], a);  // face-0 rows: fmask_idx(N,0,q) == q
+            b = fma(R.Ds[q * Np + j], ut[j], b);
+          }
+          dq[q] = cr * a + cs * b;
+        }
+#pragma unroll
+        for (int p = 0; p < Nfp; ++p) {
+          uP[p] = flip ? ut[N - p] : ut[p];
+          dnP[p] = flip ? dq[N - p] : dq[p];
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < Nfp; ++p) {
+          uP[p] = T(0);
+          dnP[p] = T(0);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) {
+        uP[p] = T(0);
+        dnP[p] = T(0);
+      }
+    }
+    // coefficients
+    const T caM = mdir ? T(1) : (mint ? T(0.5) : T(0));
+    const T cjM = mdir ? tauM : (mint ? T(0.5) * tauM : T(0));
+    const T cgM = mdir ? T(1) : (mint ? T(0.25) : T(0));
+    const T caP = pact ? T(0.5) : T(0);
+    const T cjP = pact ? T(0.5) * tauP : T(0);
+    const T cgP = pact ? T(0.25) : T(0);
+    T v1[Nfp], v2[Nfp];
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const T uM = u[fmask_idx(N, f, p)];
+      const T avgI = T(0.5) * (dnm[f][p] + dnP[p]);
+      const T jmpI = uM - uP[p];
+      const T avgM = mdir ? dnm[f][p] : avgI;
+      const T jmpM = mdir ? uM : jmpI;
+      v1[p] = -caM * avgM + cjM * jmpM - caP * avgI + cjP * jmpI;
+      v2[p] = cgM * jmpM + cgP * jmpI;
+    }
+#pragma unroll
+    for (int q = 0; q < Nfp; ++q) {
+      T a = T(0), b = T(0);
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) {
+        a = fma(R.m1d[(f * Nfp + p) * Nfp + q], v1[p], a);
+        b = fma(R.m1d[(f * Nfp + p) * Nfp + q], v2[p], b);
+      }
+      const int n = fmask_idx(N, f, q);
+      y[n] += sJ * a;
+      ex[n] -= sJ * nx * b;
+      ey[n] -= sJ * ny * b;
+    }
+  }
+  // lift: y += Dr^T (rx ex + ry ey) + Ds^T (sx ex + sy ey)
+  T tr[Np], ts[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    tr[i] = g.rx * ex[i] + g.ry * ey[i];
+    ts[i] = g.sx * ex[i] + g.sy * ey[i];
+  }
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    T a = y[i];
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      a = fma(R.Dr[j * Np + i], tr[j], a);
+      a = fma(R.Ds[j * Np + i], ts[j], a);
+    }
+    y[i] = a;
+  }
+}
+
+}  // namespace ddg

@@ -1,0 +1,684 @@
+// Kernels of the SIPG operator, its CG loop, the block-Jacobi
+// preconditioner and the right-hand-side loads, plus their host launchers.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+#include "sipg_device.cuh"
+#include "sipg_launch.h"
+
+namespace ddg {
+
+#define DDG_DEFINE_CONST(NN)                       \
+  __constant__ RefMats<NN, double> c_ref64_##NN; \
+  __constant__ RefMats<NN, float> c_ref32_##NN;
+DDG_DEFINE_CONST(1)
+DDG_DEFINE_CONST(2)
+DDG_DEFINE_CONST(3)
+DDG_DEFINE_CONST(4)
+DDG_DEFINE_CONST(5)
+
+#define DDG_CREF(NN)                                                                    \
+  template <> struct CRef<NN, double> {                                                \
+    static __device__ __forceinline__ const RefMats<NN, double>& get() { return c_ref64_##NN; } \
+  };                                                                                   \
+  template <> struct CRef<NN, float> {                                                 \
+    static __device__ __forceinline__ const RefMats<NN, float>& get() { return c_ref32_##NN; } \
+  };
+DDG_CREF(1)
+DDG_CREF(2)
+DDG_CREF(3)
+DDG_CREF(4)
+DDG_CREF(5)
+
+// ================================================================ apply
+// MODE: AM_APPLY  out0 = A in0 + alpha J M in0 + shift in0
+//       AM_PFUSE  u = in0 + beta in1 (CG direction, beta from ctl);
+//                 out1 = u; out0 = A u (+...); partial u.out0 -> ctl->pAp,
+//                 ctl->alpha = gamma / pAp  (last block)
+//       AM_RESID  out0 = in1 - (A in0 + ...); partials in1.in1, out0.out0
+//                 -> ctl->bb, ctl->rr (last block)
+template <int N, typename T, int MODE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
+  constexpr int Np = Dim<N>::Np;
+  constexpr int NT = (MODE == AM_APPLY) ? 1 : 2;
+  __shared__ __align__(128) T s_tile[NT][BLOCK * Np];
+  __shared__ int s_perm[3 * Np];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ double s_red[64];
+
+  if (MODE == AM_PFUSE && a.ctl->cont == 0) return;  // uniform across the grid
+  const int tid = threadIdx.x;
+  const int k0 = blockIdx.x * BLOCK;
+  const int nk = min(BLOCK, a.K - k0);
+  const size_t off = (size_t)k0 * Np;
+  const uint32_t bytes = (uint32_t)(nk * Np * sizeof(T));
+  const bool tma = a.use_tma && (bytes % 16u == 0u);
+
+  for (int i = tid; i < 3 * Np; i += BLOCK) s_perm[i] = a.perm[i];
+  if (tma && tid == 0) {
+    mbar_init(&s_bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tma) {
+    __shared__ int s_ok;
+    if (tid == 0) {
+      mbar_expect_tx(&s_bar, bytes * NT);
+      bulk_load(s_tile[0], a.in0 + off, bytes, &s_bar);
+      if (NT > 1) bulk_load(s_tile[NT - 1], a.in1 + off, bytes, &s_bar);
+      s_ok = mbar_wait_bounded(&s_bar, 0, &a.ctl_status[0]) ? 1 : 0;
+    }
+    __syncthreads();           // one waiter; the whole block sees its verdict
+    if (!s_ok) return;         // uniform exit: no thread is left at a barrier
+  } else {
+    for (int i = tid; i < nk * Np; i += BLOCK) {
+      s_tile[0][i] = a.in0[off + i];
+      if (NT > 1) s_tile[NT - 1][i] = a.in1[off + i];
+    }
+    __syncthreads();
+  }
+
+  const T beta = (MODE == AM_PFUSE) ? T(a.ctl->beta) : T(0);
+  const int k = k0 + tid;
+  const bool active = tid < nk;
+  T u[Np], y[Np], b2[Np];
+  double dA = 0.0, dB = 0.0;
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      if (MODE == AM_PFUSE) {
+        u[i] = s_tile[0][tid * Np + i] + beta * s_tile[1][tid * Np + i];
+      } else {
+        u[i] = s_tile[0][tid * Np + i];
+      }
+      if (MODE == AM_RESID) b2[i] = s_tile[1][tid * Np + i];
+    }
+    uint32_t w[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
+    const Geo<T> g = load_geo(a.geo, a.ldg, k);
+    if (MODE == AM_PFUSE) {
+      NbrPfuse<T, Np> src{a.in0, a.in1, beta, s_perm};
+      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src);
+    } else {
+      NbrPlain<T, Np> src{a.in0, s_perm};
+      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src);
+    }
+    if (a.shift != 0.0) {
+#pragma unroll
+      for (int i = 0; i < Np; ++i) y[i] += T(a.shift) * u[i];
+    }
+    if (MODE == AM_RESID) {
+#pragma unroll
+      for (int i = 0; i < Np; ++i) {
+        y[i] = b2[i] - y[i];
+        dA += (double)b2[i] * (double)b2[i];
+        dB += (double)y[i] * (double)y[i];
+      }
+    }
+    if (MODE == AM_PFUSE) {
+#pragma unroll
+      for (int i = 0; i < Np; ++i) dA += (double)u[i] * (double)y[i];
+    }
+  }
+  __syncthreads();  // every tile read done before the tiles are overwritten
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      s_tile[0][tid * Np + i] = y[i];
+      if (MODE == AM_PFUSE) s_tile[1][tid * Np + i] = u[i];
+    }
+  }
+  if (tma) fence_proxy_async_smem();
+  __syncthreads();
+  if (tma) {
+    if (tid == 0) {
+      bulk_store(a.out0 + off, s_tile[0], bytes);
+      if (MODE == AM_PFUSE) bulk_store(a.out1 + off, s_tile[1], bytes);
+      bulk_commit();
+      bulk_wait_read_all();
+    }
+  } else {
+    for (int i = tid; i < nk * Np; i += BLOCK) {
+      a.out0[off + i] = s_tile[0][i];
+      if (MODE == AM_PFUSE) a.out1[off + i] = s_tile[1][i];
+    }
+  }
+  if (MODE == AM_APPLY) return;
+
+  // reductions: block partials -> last block -> control block
+  block_sum2<BLOCK>(dA, dB, s_red);
+  if (tid == 0) {
+    a.partA[blockIdx.x] = dA;
+    a.partB[blockIdx.x] = dB;
+  }
+  if (!is_last_block(&a.ctl->ticket)) return;
+  double sA, sB;
+  reduce_partials2<BLOCK>(a.partA, a.partB, gridDim.x, sA, sB, s_red);
+  if (tid == 0) {
+    CgCtl* c = a.ctl;
+    if (MODE == AM_PFUSE) {
+      c->pAp = sA;
+      const double al = c->gamma / sA;
+      if (!(sA > 0.0) || !isfinite(al)) {
+        c->status = 2;  // breakdown
+        c->alpha = 0.0;
+      } else {
+        c->alpha = al;
+      }
+    } else {
+      c->bb = sA;
+      c->rr = sB;
+    }
+    c->ticket = 0u;
+  }
+}
+
+// ================================================================= CG
+// One CG step after the apply: x += alpha p; r -= alpha Ap; z = B^-1 r;
+// partials r.z, r.r -> last block: gamma, beta, iter, loop condition.
+// INIT: r given (from AM_RESID), no x/p update; zeroes p_old, sets
+// gamma0 = r.z, beta = 0, iter = 0.
+template <int N, typename T, bool PC, bool INIT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
+  constexpr int Np = Dim<N>::Np;
+  __shared__ __align__(16) T s_r[BLOCK * Np];
+  __shared__ double s_red[64];
+  if (!INIT && a.ctl->cont == 0) {
+    // the loop already stopped: make sure the while node sees 0
+    if (a.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    return;
+  }
+  const int tid = threadIdx.x;
+  const int k0 = blockIdx.x * BLOCK;
+  const int nk = min(BLOCK, a.K - k0);
+  const size_t off = (size_t)k0 * Np;
+  const T al = INIT ? T(0) : T(a.ctl->alpha);
+  double rr = 0.0, rz = 0.0;
+  for (int i = tid; i < nk * Np; i += BLOCK) {
+    T rn;
+    if (INIT) {
+      rn = a.r[off + i];
+      a.p_zero[off + i] = T(0);
+    } else {
+      a.x[off + i] += al * a.p[off + i];
+      rn = a.r[off + i] - al * a.Ap[off + i];
+      a.r[off + i] = rn;
+    }
+    rr += (double)rn * (double)rn;
+    if (PC) s_r[i] = rn;
+  }
+  if (PC) {
+    __syncthreads();
+    if (tid < nk) {
+      const int k = k0 + tid;
+      T rv[Np], zv[Np];
+#pragma unroll
+      for (int j = 0; j < Np; ++j) rv[j] = s_r[tid * Np + j];
+#pragma unroll
+      for (int i = 0; i < Np; ++i) {
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)(i * Np + j) * a.ldb + k), rv[j], acc);
+        zv[i] = acc;
+        rz += (double)rv[i] * (double)acc;
+      }
+#pragma unroll
+      for (int i = 0; i < Np; ++i) s_r[tid * Np + i] = zv[i];
+    }
+    __syncthreads();
+    for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_r[i];
+  } else {
+    rz = rr;
+  }
+  block_sum2<BLOCK>(rz, rr, s_red);
+  if (tid == 0) {
+    a.partA[blockIdx.x] = rz;
+    a.partB[blockIdx.x] = rr;
+  }
+  if (!is_last_block(&a.ctl->ticket)) return;
+  double g, r2;
+  reduce_partials2<BLOCK>(a.partA, a.partB, gridDim.x, g, r2, s_red);
+  if (tid == 0) {
+    CgCtl* c = a.ctl;
+    if (INIT) {
+      c->atol2 = fmax(c->tol2 * c->bb, c->atol_sq);
+      c->beta = 0.0;
+      c->iter = 0;
+      c->status = 0;
+    } else {
+      c->beta = g / c->gamma;
+      c->iter += 1;
+    }
+    c->gamma = g;
+    c->rr = r2;
+    const double rs = c->use_pc ? r2 : g;
+    int cont = (rs > c->atol2) && (c->iter < c->maxiter) && (c->status == 0);
+    if (!isfinite(g) || !isfinite(r2)) {
+      c->status = 2;
+      cont = 0;
+    }
+    if (!INIT && !isfinite(c->beta)) {
+      c->status = 2;
+      cont = 0;
+    }
+    if (a.dev_status && *(volatile const unsigned int*)a.dev_status != 0u) {
+      c->status = 3;  // a kernel reported a device-side error: stop now
+      cont = 0;
+    }
+    if (cont == 0 && c->status == 0 && rs > c->atol2) c->status = 1;  // maxiter
+    c->cont = cont;
+    c->ticket = 0u;
+    if (a.has_cond) cudaGraphSetConditional(a.cond, (unsigned)cont);
+  }
+}
+
+// ========================================================= block Jacobi
+// Self block column j of element k = (local operator with zero neighbour
+// values) applied to e_j: the coloured probe of sipg.py:671-704 without
+// the colouring.  Output blocks[k][i][j] (row-major per element, float64).
+template <int N, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_self_blocks(BlockArgs a) {
+  constexpr int Np = Dim<N>::Np;
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k >= a.K) return;
+  uint32_t w[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
+  const Geo<double> g = load_geo(a.geo, a.ldg, k);
+  NbrZero<double, Np> src;
+  for (int j = 0; j < Np; ++j) {
+    double u[Np], y[Np];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) u[i] = (i == j) ? 1.0 : 0.0;
+    elem_apply<N, double, false>(u, y, g, w, a.geo, a.ldg, a.tau, a.alpha, src);
+#pragma unroll
+    for (int i = 0; i < Np; ++i) a.blocks[(size_t)k * Np * Np + i * Np + j] = y[i] + (i == j ? a.shift : 0.0);
+  }
+}
+
+// Gauss-Jordan inverse with partial pivoting per element; writes the
+// inverse structure-of-arrays binv[(i Np + j) ldb + k] in float64 and float32.
+template <int N, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_invert_blocks(BlockArgs a) {
+  constexpr int Np = Dim<N>::Np;
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k >= a.K) return;
+  double m[Np][2 * Np];
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) {
+      m[i][j] = a.blocks[(size_t)k * Np * Np + i * Np + j];
+      m[i][Np + j] = (i == j) ? 1.0 : 0.0;
+    }
+  bool ok = true;
+  for (int c = 0; c < Np; ++c) {
+    int piv = c;
+    double best = fabs(m[c][c]);
+    for (int i = c + 1; i < Np; ++i)
+      if (fabs(m[i][c]) > best) {
+        best = fabs(m[i][c]);
+        piv = i;
+      }
+    if (!(best > 0.0)) {
+      ok = false;
+      break;
+    }
+    if (piv != c)
+      for (int j = 0; j < 2 * Np; ++j) {
+        const double t = m[c][j];
+        m[c][j] = m[piv][j];
+        m[piv][j] = t;
+      }
+    const double inv = 1.0 / m[c][c];
+    for (int j = 0; j < 2 * Np; ++j) m[c][j] *= inv;
+    for (int i = 0; i < Np; ++i) {
+      if (i == c) continue;
+      const double fct = m[i][c];
+      if (fct != 0.0)
+        for (int j = 0; j < 2 * Np; ++j) m[i][j] -= fct * m[c][j];
+    }
+  }
+  if (!ok) atomicOr(a.status, ST_BAD_INDEX);
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) {
+      const double v = ok ? m[i][Np + j] : NAN;
+      a.binv64[(size_t)(i * Np + j) * a.ldb + k] = v;
+      a.binv32[(size_t)(i * Np + j) * a.ldb + k] = (float)v;
+    }
+}
+
+// z = B^-1 r for every element (the standalone preconditioner callable).
+template <int N, typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pc_apply(const T* __restrict__ r, T* __restrict__ z,
+                                                      const T* __restrict__ binv, int ldb, int K) {
+  constexpr int Np = Dim<N>::Np;
+  __shared__ __align__(16) T s[BLOCK * Np];
+  const int tid = threadIdx.x, k0 = blockIdx.x * BLOCK, nk = min(BLOCK, K - k0);
+  const size_t off = (size_t)k0 * Np;
+  for (int i = tid; i < nk * Np; i += BLOCK) s[i] = r[off + i];
+  __syncthreads();
+  if (tid < nk) {
+    const int k = k0 + tid;
+    T rv[Np];
+#pragma unroll
+    for (int j = 0; j < Np; ++j) rv[j] = s[tid * Np + j];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      T acc = T(0);
+#pragma unroll
+      for (int j = 0; j < Np; ++j) acc = fma(__ldg(binv + (size_t)(i * Np + j) * ldb + k), rv[j], acc);
+      s[tid * Np + i] = acc;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < nk * Np; i += BLOCK) z[off + i] = s[i];
+}
+
+// ================================================================ RHS
+// rhs = J M f - L_D(u_dir) + L_N(q_neu)   (sipg.py:852-864, 398-453)
+template <int N, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_rhs(RhsArgs a) {
+  constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k >= a.K) return;
+  const RefMats<N, double>& R = CRef<N, double>::get();
+  const Geo<double> g = load_geo(a.geo, a.ldg, k);
+  double y[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) y[i] = 0.0;
+  if (a.f) {
+    double fv[Np];
+#pragma unroll
+    for (int j = 0; j < Np; ++j) fv[j] = a.f[(size_t)k * Np + j];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < Np; ++j) s = fma(R.M[i * Np + j], fv[j], s);
+      y[i] = g.J * s;
+    }
+  }
+  uint32_t w[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
+  if (a.u_dir) {
+    // Dirichlet load with u = 0: only Dirichlet-tagged faces contribute.
+    double yd[Np], ex[Np], ey[Np];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) yd[i] = ex[i] = ey[i] = 0.0;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (((w[f] >> 3) & 3) != 1) continue;
+      const double sJ = g.sJ[f], tauM = a.tau * sJ / g.J;
+      double ud[Nfp];
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) ud[p] = a.u_dir[(size_t)k * Np + fmask_idx(N, f, p)];
+#pragma unroll
+      for (int q = 0; q < Nfp; ++q) {
+        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int p = 0; p < Nfp; ++p) {
+          const double m = R.m1d[(f * Nfp + p) * Nfp + q];
+          s1 = fma(m, -tauM * ud[p], s1);
+          s2 = fma(m, -ud[p], s2);
+        }
+        const int n = fmask_idx(N, f, q);
+        yd[n] += sJ * s1;
+        ex[n] -= sJ * g.nx[f] * s2;
+        ey[n] -= sJ * g.ny[f] * s2;
+      }
+    }
+    double tr[Np], ts[Np];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      tr[i] = g.rx * ex[i] + g.ry * ey[i];
+      ts[i] = g.sx * ex[i] + g.sy * ey[i];
+    }
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      double s = yd[i];
+#pragma unroll
+      for (int j = 0; j < Np; ++j) {
+        s = fma(R.Dr[j * Np + i], tr[j], s);
+        s = fma(R.Ds[j * Np + i], ts[j], s);
+      }
+      y[i] -= s;
+    }
+  }
+  if (a.q_neu) {
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (((w[f] >> 3) & 3) != 2) continue;
+      double q[Nfp];
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) q[p] = a.q_neu[(size_t)k * 3 * Nfp + f * Nfp + p];
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) {
+        double s = 0.0;
+#pragma unroll
+        for (int qq = 0; qq < Nfp; ++qq) s = fma(R.m1d[(f * Nfp + p) * Nfp + qq], q[qq], s);
+        y[fmask_idx(N, f, p)] += g.sJ[f] * s;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < Np; ++i) a.rhs[(size_t)k * Np + i] = y[i];
+}
+
+// ============================================================ vectors
+__global__ void k_axpby(int64_t n, double al, const double* __restrict__ x, double be, double* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = al * x[i] + be * y[i];
+}
+template <typename S, typename D>
+__global__ void k_cast(int64_t n, const S* __restrict__ s, D* __restrict__ d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (D)s[i];
+}
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_dot(int64_t n, const T* __restrict__ x, const T* __restrict__ y,
+                                                double* part, unsigned int* ticket, double* out) {
+  __shared__ double s_red[64];
+  double s = 0.0, d = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * BLOCK)
+    s += (double)x[i] * (double)y[i];
+  block_sum2<BLOCK>(s, d, s_red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (!is_last_block(ticket)) return;
+  double t, u;
+  reduce_partials2<BLOCK>(part, nullptr, gridDim.x, t, u, s_red);
+  if (threadIdx.x == 0) {
+    *out = t;
+    *ticket = 0u;
+  }
+}
+
+// ============================================================ launchers
+template <int N, typename T> struct CRefSym;
+#define DDG_SYM(NN)                                                                        \
+  template <> struct CRefSym<NN, double> { static const void* sym() { return &c_ref64_##NN; } }; \
+  template <> struct CRefSym<NN, float> { static const void* sym() { return &c_ref32_##NN; } };
+DDG_SYM(1)
+DDG_SYM(2)
+DDG_SYM(3)
+DDG_SYM(4)
+DDG_SYM(5)
+
+namespace {
+template <int N, typename T>
+cudaError_t upload_one(const double* Dr, const double* Ds, const double* M, const double* m1d) {
+  constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
+  RefMats<N, T> h;
+  for (int i = 0; i < Np * Np; ++i) {
+    h.Dr[i] = (T)Dr[i];
+    h.Ds[i] = (T)Ds[i];
+    h.M[i] = (T)M[i];
+  }
+  for (int i = 0; i < 3 * Nfp * Nfp; ++i) h.m1d[i] = (T)m1d[i];
+  return cudaMemcpyToSymbol(CRefSym<N, T>::sym(), &h, sizeof(h));
+}
+}  // namespace
+
+
+
+template <int N>
+static cudaError_t upload_n(const double* Dr, const double* Ds, const double* M, const double* m1d) {
+  cudaError_t e = upload_one<N, double>(Dr, Ds, M, m1d);
+  if (e != cudaSuccess) return e;
+  return upload_one<N, float>(Dr, Ds, M, m1d);
+}
+
+cudaError_t upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d) {
+  switch (N) {
+    case 1: return upload_n<1>(Dr, Ds, M, m1d);
+    case 2: return upload_n<2>(Dr, Ds, M, m1d);
+    case 3: return upload_n<3>(Dr, Ds, M, m1d);
+    case 4: return upload_n<4>(Dr, Ds, M, m1d);
+    case 5: return upload_n<5>(Dr, Ds, M, m1d);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T> constexpr int apply_block() { return sizeof(T) == 8 ? 128 : 128; }
+
+template <int N, typename T>
+static cudaError_t launch_apply_n(int mode, const ApplyArgs<T>& a, cudaStream_t s) {
+  constexpr int B = apply_block<T>();
+  const int grid = (a.K + B - 1) / B;
+  switch (mode) {
+    case AM_APPLY: k_apply<N, T, AM_APPLY, B><<<grid, B, 0, s>>>(a); break;
+    case AM_PFUSE: k_apply<N, T, AM_PFUSE, B><<<grid, B, 0, s>>>(a); break;
+    case AM_RESID: k_apply<N, T, AM_RESID, B><<<grid, B, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_apply(int N, int mode, const ApplyArgs<T>& a, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_apply_n<1, T>(mode, a, s);
+    case 2: return launch_apply_n<2, T>(mode, a, s);
+    case 3: return launch_apply_n<3, T>(mode, a, s);
+    case 4: return launch_apply_n<4, T>(mode, a, s);
+    case 5: return launch_apply_n<5, T>(mode, a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+template cudaError_t launch_apply<double>(int, int, const ApplyArgs<double>&, cudaStream_t);
+template cudaError_t launch_apply<float>(int, int, const ApplyArgs<float>&, cudaStream_t);
+
+int apply_grid(int K) { return (K + 127) / 128; }
+int cg_grid(int K) { return (K + 127) / 128; }
+
+template <int N, typename T>
+static cudaError_t launch_cg_n(bool pc, bool init, const CgArgs<T>& a, cudaStream_t s) {
+  constexpr int B = 128;
+  const int grid = (a.K + B - 1) / B;
+  if (pc) {
+    if (init) k_cg_step<N, T, true, true, B><<<grid, B, 0, s>>>(a);
+    else k_cg_step<N, T, true, false, B><<<grid, B, 0, s>>>(a);
+  } else {
+    if (init) k_cg_step<N, T, false, true, B><<<grid, B, 0, s>>>(a);
+    else k_cg_step<N, T, false, false, B><<<grid, B, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_cg_step(int N, bool pc, bool init, const CgArgs<T>& a, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_cg_n<1, T>(pc, init, a, s);
+    case 2: return launch_cg_n<2, T>(pc, init, a, s);
+    case 3: return launch_cg_n<3, T>(pc, init, a, s);
+    case 4: return launch_cg_n<4, T>(pc, init, a, s);
+    case 5: return launch_cg_n<5, T>(pc, init, a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+template cudaError_t launch_cg_step<double>(int, bool, bool, const CgArgs<double>&, cudaStream_t);
+template cudaError_t launch_cg_step<float>(int, bool, bool, const CgArgs<float>&, cudaStream_t);
+
+template <int N>
+static cudaError_t launch_blocks_n(const BlockArgs& a, cudaStream_t s) {
+  constexpr int B = 64;
+  const int grid = (a.K + B - 1) / B;
+  k_self_blocks<N, B><<<grid, B, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_invert_blocks<N, B><<<grid, B, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_block_jacobi(int N, const BlockArgs& a, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_blocks_n<1>(a, s);
+    case 2: return launch_blocks_n<2>(a, s);
+    case 3: return launch_blocks_n<3>(a, s);
+    case 4: return launch_blocks_n<4>(a, s);
+    case 5: return launch_blocks_n<5>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int N, typename T>
+static cudaError_t launch_pc_n(const T* r, T* z, const T* binv, int ldb, int K, cudaStream_t s) {
+  constexpr int B = 128;
+  k_pc_apply<N, T, B><<<(K + B - 1) / B, B, 0, s>>>(r, z, binv, ldb, K);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_pc_apply(int N, const T* r, T* z, const T* binv, int ldb, int K, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_pc_n<1, T>(r, z, binv, ldb, K, s);
+    case 2: return launch_pc_n<2, T>(r, z, binv, ldb, K, s);
+    case 3: return launch_pc_n<3, T>(r, z, binv, ldb, K, s);
+    case 4: return launch_pc_n<4, T>(r, z, binv, ldb, K, s);
+    case 5: return launch_pc_n<5, T>(r, z, binv, ldb, K, s);
+  }
+  return cudaErrorInvalidValue;
+}
+template cudaError_t launch_pc_apply<double>(int, const double*, double*, const double*, int, int, cudaStream_t);
+template cudaError_t launch_pc_apply<float>(int, const float*, float*, const float*, int, int, cudaStream_t);
+
+template <int N>
+static cudaError_t launch_rhs_n(const RhsArgs& a, cudaStream_t s) {
+  constexpr int B = 128;
+  k_rhs<N, B><<<(a.K + B - 1) / B, B, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs(int N, const RhsArgs& a, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_rhs_n<1>(a, s);
+    case 2: return launch_rhs_n<2>(a, s);
+    case 3: return launch_rhs_n<3>(a, s);
+    case 4: return launch_rhs_n<4>(a, s);
+    case 5: return launch_rhs_n<5>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+static int vec_grid(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  return (int)(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
+}
+cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, double* y, cudaStream_t s) {
+  k_axpby<<<vec_grid(n), 256, 0, s>>>(n, al, x, be, y);
+  return cudaGetLastError();
+}
+cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s) {
+  if (to_prec == 1) k_cast<double, float><<<vec_grid(n), 256, 0, s>>>(n, (const double*)src, (float*)dst);
+  else k_cast<float, double><<<vec_grid(n), 256, 0, s>>>(n, (const float*)src, (double*)dst);
+  return cudaGetLastError();
+}
+int dot_grid(int64_t n) { return vec_grid(n); }
+cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double* part, unsigned int* ticket,
+                       double* out, cudaStream_t s) {
+  const int g = vec_grid(n);
+  if (prec == 0) k_dot<double, 256><<<g, 256, 0, s>>>(n, (const double*)x, (const double*)y, part, ticket, out);
+  else k_dot<float, 256><<<g, 256, 0, s>>>(n, (const float*)x, (const float*)y, part, ticket, out);
+  return cudaGetLastError();
+}
+
+}  // namespace ddg

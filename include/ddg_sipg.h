@@ -1,0 +1,187 @@
+/*
+ * ddg_sipg.h -- C ABI of the B200 (sm_100a) matrix-free SIPG
+ * Poisson/Helmholtz solver.
+ *
+ * Plain C: pointers, sizes and int status codes.  No C++ or torch types
+ * cross this boundary and no exception escapes it.  Every entry point
+ * returns DDG_OK (0) on success; ddg_last_error() gives the message of the
+ * last failure on the calling thread.
+ *
+ * Layouts follow ddg (reference project CorbinFoucart/ddg):
+ *   volume vectors  element-major flat, index k*Np + n (u.T.reshape(-1) of
+ *                   an (Np, K) field)        -- src/ddg/dg2d/sipg.py:204
+ *   face vectors    index k*3*Nfp + f*Nfp + p (order='F' of (3 Nfp, K))
+ *                                            -- src/ddg/dg2d/sipg.py:442
+ *   bc_types        (K, 3) int32, 0 interior / 1 Dirichlet / 2 Neumann
+ *                                            -- src/ddg/dg2d/sipg.py:53-56
+ * Device vectors are caller-owned device memory on the handle's device.
+ * One handle is used by one stream at a time.
+ */
+#ifndef DDG_SIPG_H
+#define DDG_SIPG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define DDG_OK               0
+#define DDG_ERR_INVALID      1   /* bad argument / inconsistent mesh        */
+#define DDG_ERR_CUDA         2   /* a CUDA runtime call failed              */
+#define DDG_ERR_UNSUPPORTED  3   /* degree or option not built              */
+#define DDG_ERR_NOMEM        4   /* device allocation failed / over budget  */
+#define DDG_ERR_DEVICE       5   /* a kernel reported an error (timeout,    */
+                                 /* bad index) through its status word      */
+
+/* ---- BC codes (src/ddg/dg2d/sipg.py:53-56) ---------------------------- */
+#define DDG_BC_INTERIOR  0
+#define DDG_BC_DIRICHLET 1
+#define DDG_BC_NEUMANN   2
+
+/* ---- precisions of the operator apply -------------------------------- */
+#define DDG_FP64 0
+#define DDG_FP32 1
+
+/* ---- solver status (jax's cg discards its info; we return one) -------- */
+#define DDG_SOLVE_CONVERGED  0
+#define DDG_SOLVE_MAXITER    1
+#define DDG_SOLVE_BREAKDOWN  2   /* p.Ap <= 0 or non-finite scalar */
+#define DDG_SOLVE_DEVICE_ERR 3   /* a kernel reported an error; loop stopped */
+
+/* Highest polynomial degree with built kernels. */
+#define DDG_MAX_DEGREE 5
+
+typedef struct ddg_sipg_op ddg_sipg_op;      /* opaque, library-owned */
+
+/*
+ * Mesh + operator description for ddg_sipg_create.  All pointers are HOST
+ * memory and are only read during the call.
+ *
+ * Replaces the Mesh2D fields the reference's sipg_bilinear_form reads
+ * (src/ddg/dg2d/mesh.py:50-101, src/ddg/dg2d/sipg.py:168-263): the
+ * reference-element matrices, per-element affine geometry, connectivity,
+ * node maps and BC tags.  Geometry is per element (straight-sided
+ * triangles: rx..J are constant per element), taken at each element's first
+ * node / each face's first node exactly as sipg.py:261-263 takes sJ, Fscale.
+ */
+typedef struct {
+    int32_t N;             /* polynomial degree, 1..DDG_MAX_DEGREE          */
+    int32_t K;             /* number of elements                            */
+    int32_t device;        /* CUDA device ordinal                           */
+    int32_t reserved;
+    double  tau_scale;     /* penalty tau = tau_scale (N+1)^2 sJ/J          */
+    const double *Dr, *Ds; /* (Np, Np) row-major                            */
+    const double *M;       /* (Np, Np) reference mass inv(V V^T)            */
+    const double *m1d;     /* (3, Nfp, Nfp) face masses (sipg.py:98-110)    */
+    const int64_t *Fmask;  /* (Nfp, 3)                                      */
+    const int64_t *rot_perm; /* (3, Np): node of the element re-labelled so
+                                that its face f is face 0                    */
+    const double *geo;     /* (K, 14): rx sx ry sy J, then for f=0..2:
+                              nx_f ny_f sJ_f                                */
+    const int64_t *EToE, *EToF;   /* (K, 3)                                 */
+    const int64_t *vmapM, *vmapP; /* (3 Nfp K)                              */
+    const int32_t *bc_types;      /* (K, 3)                                 */
+} ddg_sipg_mesh_desc;
+
+/* Build the device-resident operator.  Replaces the per-call setup of
+ * src/ddg/dg2d/sipg.py:849-850 (_local_mass / _face_1d_mass_matrices) and
+ * the mesh fields above.  Allocates device memory owned by the handle. */
+int ddg_sipg_create(const ddg_sipg_mesh_desc *desc, ddg_sipg_op **out);
+int ddg_sipg_destroy(ddg_sipg_op *op);
+
+/* Change the BC tags of an existing handle (same mesh). */
+int ddg_sipg_set_bc(ddg_sipg_op *op, const int32_t *bc_types);
+
+/* y = A u + alpha * J (M_ref u).
+ * Replaces sipg_apply_2d(mesh, u, bc_types=..., u_dir=None) of
+ * src/ddg/dg2d/sipg.py:304-337 (alpha = 0) and the Helmholtz matvec
+ * src/ddg/dg2d/sipg.py:589-601 / multigrid.py:53-74 (alpha > 0).
+ * u, y: device, K*Np elements of double (DDG_FP64) or float (DDG_FP32). */
+int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
+                   const void *u, void *y, void *stream);
+
+/* rhs = J (M_ref f) - L_D(u_dir) + L_N(q_neu), all float64 device vectors.
+ * Replaces the RHS assembly of src/ddg/dg2d/sipg.py:852-864 with
+ * sipg_dirichlet_load_2d (:398-417) and sipg_neumann_load_2d (:420-453).
+ * f may be NULL (zero source), u_dir NULL (no Dirichlet load), q_neu NULL. */
+int ddg_sipg_rhs(ddg_sipg_op *op, const double *f, const double *u_dir,
+                 const double *q_neu, double *rhs, void *stream);
+
+/* Block-Jacobi preconditioner of alpha M + A: per-element (Np, Np) diagonal
+ * blocks, inverted on the device.  Replaces extract_block_diag_matfree +
+ * _block_jacobi_apply (src/ddg/dg2d/sipg.py:671-715) and the two builders
+ * make_sipg/helmholtz_block_jacobi_preconditioner (:718-805). */
+int ddg_sipg_pc_build(ddg_sipg_op *op, double alpha, void *stream);
+/* z = B^-1 r on device vectors (the M^-1(v_flat) callable, sipg.py:711-713). */
+int ddg_sipg_pc_apply(ddg_sipg_op *op, int precision, const void *r, void *z,
+                      void *stream);
+/* Copy the (K, Np, Np) float64 diagonal blocks (not inverted) to device
+ * memory `blocks` (for tests; the inverse is kept internally). */
+int ddg_sipg_pc_blocks(ddg_sipg_op *op, double *blocks, void *stream);
+
+/* ---- Krylov solve ----------------------------------------------------- */
+#define DDG_PC_NONE   0
+#define DDG_PC_JACOBI 1   /* block-Jacobi from ddg_sipg_pc_build           */
+#define DDG_PC_USER   2   /* reserved                                       */
+
+typedef struct {
+    double  tol;        /* relative tolerance (IterativeConfig.tol)         */
+    double  atol;       /* absolute tolerance (IterativeConfig.atol)        */
+    int32_t maxiter;    /* IterativeConfig.maxiter                          */
+    int32_t pc;         /* DDG_PC_*                                          */
+    double  alpha;      /* Helmholtz mass coefficient (0 = Poisson)         */
+    double  shift;      /* extra  shift * I  (singular-Poisson eps-shift)   */
+    int32_t precision;  /* DDG_FP64 or DDG_FP32 (vectors and operator)      */
+    int32_t reserved;
+} ddg_cg_config;
+
+typedef struct {
+    int32_t status;      /* DDG_SOLVE_*                                     */
+    int32_t iterations;
+    double  res_norm2;   /* final r.r (preconditioned: r.r; else r.z = r.r) */
+    double  b_norm2;     /* b.b                                             */
+} ddg_solve_info;
+
+/* CG on (alpha M + A + shift I) x = b with the stopping rule of
+ * jax.scipy.sparse.linalg.cg as called at src/ddg/dg2d/sipg.py:604,910:
+ * r.r <= max(tol^2 b.b, atol^2) checked before each iteration, at most
+ * maxiter iterations.  b, x: device vectors of the config's precision;
+ * x holds x0 on entry and the solution on exit.  The whole loop runs on the
+ * device as a CUDA graph with a conditional while node; the call returns
+ * after the stream has been synchronised and `info` filled. */
+int ddg_sipg_cg(ddg_sipg_op *op, const ddg_cg_config *cfg, const void *b,
+                void *x, void *stream, ddg_solve_info *info);
+
+/* ---- small vector helpers (device) ------------------------------------ */
+/* y = a*x + b*y  (float64) */
+int ddg_axpby(int64_t n, double a, const double *x, double b, double *y, void *stream);
+/* out[0] = x.y  (float64 accumulation), out device double */
+int ddg_dot(int64_t n, int precision, const void *x, const void *y, double *out, void *stream);
+/* float64 <-> float32 copies */
+int ddg_cast(int64_t n, int to_precision, const void *src, void *dst, void *stream);
+
+/* ---- mesh connectivity (host, C++) ------------------------------------ */
+/* EToE/EToF as src/ddg/dg2d/mesh.py:520-571 (_ti_connect_2d), bit-exact:
+ * face keys v_min*n_nodes+v_max, stable sort, adjacent equal keys pair,
+ * boundary faces point to themselves.  EToV (K,3) int64 host.            */
+int ddg_mesh_connect(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *EToF);
+/* vmapM/vmapP as src/ddg/dg2d/mesh.py:574-627 (_build_maps_2d), bit-exact:
+ * first face node of the partner within node_tol * edge length, fallback
+ * vmapM.  x, y: (Np, K) row-major (the reference's arrays), Fmask (Nfp,3). */
+int ddg_mesh_maps(int64_t K, int32_t N, const int64_t *Fmask,
+                  const double *x, const double *y,
+                  const int64_t *EToE, const int64_t *EToF,
+                  const int64_t *EToV, const double *VX, const double *VY,
+                  double node_tol, int64_t *vmapM, int64_t *vmapP);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *ddg_last_error(void);
+/* Library version string. */
+const char *ddg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDG_SIPG_H */

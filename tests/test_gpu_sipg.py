@@ -1,0 +1,297 @@
+"""GPU parity of the SIPG operator, loads, block-Jacobi and CG against the
+CPU oracle (tolerances in each test), plus the reference's manufactured-
+solution tests run through the product API."""
+
+import numpy as np
+import pytest
+
+from oracle import mesh as om
+from oracle import refinement as orf
+from oracle import sipg as osp
+
+pytestmark = pytest.mark.gpu
+
+APPLY_RTOL64 = 1e-12       # float64 operator vs oracle (max-abs relative)
+APPLY_RTOL32 = 2e-5        # float32 operator vs oracle
+
+
+def _pair(Kx, Ky, N, x1=1.0, y1=1.0):
+    from ddg_b200.dg2d import mesh as pm
+    VX, VY, E = om.uniform_rectangle_mesh_2d(0.0, x1, 0.0, y1, Kx, Ky)
+    return om.build_mesh_2d(VX, VY, E, N), pm.build_mesh_2d(VX, VY, E, N)
+
+
+def _refined_pair(N):
+    from ddg_b200.dg2d import mesh as pm
+    f = orf.UniformForest(*om.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 2.0, 2, 3), N)
+    f.refine_all()
+    f.refine_all()
+    a = f.active()
+    return om.build_mesh_2d(*a, N), pm.build_mesh_2d(*a, N)
+
+
+def _bcs(m):
+    K = m.K
+    isb = m.EToE == np.arange(K)[:, None]
+    nx = m.nx.reshape((m.Nfp, 3, K), order="F")[0].T
+    out = {
+        "dirichlet": np.where(isb, 1, 0).astype(np.int32),
+        "neumann": np.where(isb, 2, 0).astype(np.int32),
+        "mixed": np.where(isb, np.where(np.abs(nx) > 0.5, 1, 2), 0).astype(np.int32),
+        "interior_tagged_boundary": np.zeros((K, 3), dtype=np.int32),
+    }
+    return out
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("bcname", ["dirichlet", "neumann", "mixed", "interior_tagged_boundary"])
+def test_apply_fp64_matches_oracle(N, bcname):
+    from ddg_b200.dg2d.sipg import sipg_apply_2d
+    o, p = _pair(5, 4, N)
+    bc = _bcs(o)[bcname]
+    rng = np.random.default_rng(N)
+    u = rng.standard_normal((o.Np, o.K))
+    for tau in (200.0, 0.5):
+        ref = osp.apply(o, u, bc_types=bc, tau_scale=tau)
+        got = sipg_apply_2d(p, u, bc_types=bc, tau_scale=tau)
+        assert _rel(got, ref) < APPLY_RTOL64, (N, bcname, tau)
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_apply_refined_mesh_and_helmholtz(N):
+    import torch
+    o, p = _refined_pair(N)
+    bc = osp.boundary_bc(o)
+    op = p.device_operator(bc, 200.0)
+    u = np.random.default_rng(7).standard_normal((o.Np, o.K))
+    for alpha in (0.0, 5.0):
+        ref = osp.flat_op(o, bc_types=bc, alpha=alpha)(u.T.reshape(-1))
+        got = op.apply(torch.as_tensor(u.T.reshape(-1), device="cuda"), alpha=alpha).cpu().numpy()
+        assert _rel(got, ref) < APPLY_RTOL64
+
+
+@pytest.mark.parametrize("N", [1, 3, 4])
+def test_apply_fp32_matches_oracle(N):
+    import torch
+    o, p = _pair(6, 5, N)
+    bc = _bcs(o)["mixed"]
+    op = p.device_operator(bc, 200.0)
+    u = np.random.default_rng(3).standard_normal((o.Np, o.K))
+    ref = osp.flat_op(o, bc_types=bc, alpha=3.0)(u.T.reshape(-1))
+    got = op.apply(torch.as_tensor(u.T.reshape(-1), dtype=torch.float32, device="cuda"), alpha=3.0)
+    assert _rel(got.double().cpu().numpy(), ref) < APPLY_RTOL32
+
+
+def test_apply_ragged_tail_and_unaligned_pointer():
+    """K not a multiple of the tile and a vector that is not 16-byte aligned
+    take the plain-load path; results must not change."""
+    import torch
+    o, p = _pair(7, 3, 3)        # K = 42
+    bc = _bcs(o)["dirichlet"]
+    op = p.device_operator(bc, 200.0)
+    u = np.random.default_rng(1).standard_normal(o.Np * o.K)
+    ref = osp.flat_op(o, bc_types=bc)(u)
+    buf = torch.zeros(u.size + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.as_tensor(u, device="cuda")
+    out = torch.zeros(u.size + 1, dtype=torch.float64, device="cuda")
+    op.apply(buf[1:], out=out[1:])
+    assert _rel(out[1:].cpu().numpy(), ref) < APPLY_RTOL64
+
+
+def test_loads_match_oracle():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 6, 4)
+    bc = _bcs(o)["mixed"]
+    rng = np.random.default_rng(11)
+    ud = rng.standard_normal((o.Np, o.K))
+    q = rng.standard_normal((3 * o.Nfp, o.K))
+    assert _rel(ps.sipg_dirichlet_load_2d(p, ud, bc_types=bc), osp.dirichlet_load(o, ud, bc_types=bc)) < 1e-12
+    assert _rel(ps.sipg_neumann_load_2d(p, q, bc_types=bc), osp.neumann_load(o, q, bc_types=bc)) < 1e-12
+    u = rng.standard_normal((o.Np, o.K))
+    ref = osp.apply(o, u, bc_types=bc, u_dir=ud)
+    assert _rel(ps.sipg_apply_2d(p, u, bc_types=bc, u_dir=ud), ref) < 1e-12
+
+
+@pytest.mark.parametrize("alpha", [0.0, 37.0])
+def test_block_jacobi_blocks_and_apply(alpha):
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(8, 8, 3)
+    bc = osp.boundary_bc(o)
+    A = osp.dense_matrix(o, bc_types=bc, alpha=alpha)
+    ref_blocks = osp.extract_block_diag_dense(A, o.Np, o.K)
+    pc = (ps.make_sipg_block_jacobi_preconditioner(p, bc_types=bc) if alpha == 0.0 else
+          ps.make_helmholtz_block_jacobi_preconditioner(p, alpha=alpha, nu=0.01, bc_types=bc))
+    got = pc.blocks().cpu().numpy()
+    assert np.max(np.abs(got - ref_blocks)) < 1e-11 * max(1.0, np.max(np.abs(ref_blocks)))
+    v = np.random.default_rng(0).standard_normal(o.Np * o.K)
+    z_ref = osp.block_jacobi_from_blocks(ref_blocks)(v)
+    assert np.max(np.abs(pc(v) - z_ref)) < 1e-11 * max(1.0, np.max(np.abs(z_ref)))
+    assert float(v @ pc(v)) > 0.0
+
+
+@pytest.mark.parametrize("use_pc", [False, True])
+def test_cg_matches_oracle_cg(use_pc):
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(8, 8, 3)
+    bc = osp.boundary_bc(o)
+    src = np.random.default_rng(4).standard_normal((o.Np, o.K))
+    cfg_o = osp.IterativeConfig(tol=1e-10, maxiter=3000)
+    pco = osp.make_block_jacobi(o, bc_types=bc) if use_pc else None
+    u_ref, it_ref = osp.solve_poisson(o, src, bc_types=bc, iterative=cfg_o, preconditioner=pco, return_info=True)
+    pcp = ps.make_sipg_block_jacobi_preconditioner(p, bc_types=bc) if use_pc else None
+    u, info = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=ps.IterativeConfig(tol=1e-10, maxiter=3000),
+                                       preconditioner=pcp, return_info=True)
+    assert info.status == "converged"
+    # long CG runs are rounding-sensitive: counts agree to a few percent
+    assert abs(info.iterations - it_ref) <= max(2, 0.03 * it_ref)
+    assert _rel(u, u_ref) < 1e-8
+
+
+def test_cg_x0_and_maxiter_and_atol():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 6, 2)
+    bc = osp.boundary_bc(o)
+    src = np.random.default_rng(5).standard_normal((o.Np, o.K))
+    u1, i1 = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=ps.IterativeConfig(tol=1e-12, maxiter=5000),
+                                      return_info=True)
+    u2, i2 = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=ps.IterativeConfig(tol=1e-12, maxiter=5000),
+                                      x0=u1, return_info=True)
+    assert i2.iterations <= 5 and _rel(u2, u1) < 1e-10
+    _, i3 = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=ps.IterativeConfig(tol=1e-14, maxiter=7),
+                                     return_info=True)
+    assert i3.iterations == 7 and i3.status == "maxiter"
+    _, i4 = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=ps.IterativeConfig(tol=0.0, atol=1e30),
+                                     return_info=True)
+    assert i4.iterations == 0
+
+
+# ----------------- the reference's own solve tests, through the product API
+
+def _rel_l2(m, u, ue):
+    return float(np.sqrt(np.sum(m.J * (u - ue) ** 2) / np.sum(m.J * ue ** 2)))
+
+
+@pytest.mark.parametrize("N,Kx,Ky", [(3, 6, 6), (3, 10, 10), (4, 8, 8)])
+def test_full_dirichlet_manufactured(N, Kx, Ky):
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(Kx, Ky, N)
+    bc = _bcs(o)["dirichlet"]
+    ue = np.sin(np.pi * p.x) * np.sin(np.pi * p.y)
+    u_lu = ps.solve_sipg_poisson_2d(p, 2 * np.pi ** 2 * ue, bc_types=bc)
+    u_cg = ps.solve_sipg_poisson_2d(p, 2 * np.pi ** 2 * ue, bc_types=bc,
+                                    iterative=ps.IterativeConfig(tol=1e-12, maxiter=4000))
+    assert _rel_l2(p, u_lu, ue) < 1e-3 and _rel_l2(p, u_cg, ue) < 1e-3
+    assert np.max(np.abs(u_cg - u_lu)) < 1e-8
+
+
+def test_mixed_nonhomog_neumann_and_harmonic_dirichlet():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(8, 8, 3)
+    ue = p.x * (1 - p.x) * p.y
+    xf = p.x.reshape(-1, order="F")[p.vmapM]
+    q = (xf * (1 - xf)).reshape((3 * p.Nfp, p.K), order="F")
+    ny = p.ny.reshape((p.Nfp, 3, p.K), order="F")[0]
+    yf = np.stack([p.y[p.Fmask[:, f], :].mean(axis=0) for f in range(3)])
+    isb = (p.EToE == np.arange(p.K)[:, None]).T
+    neu = isb & (np.abs(ny) > 0.5) & (yf > 0.5)
+    bc = np.where(isb & ~neu, 1, np.where(neu, 2, 0)).T.astype(np.int32)
+    cfg = ps.IterativeConfig(tol=1e-12, maxiter=4000)
+    u = ps.solve_sipg_poisson_2d(p, 2.0 * p.y, bc_types=bc, q_neu=q, iterative=cfg)
+    assert _rel_l2(p, u, ue) < 1e-3
+    uh = p.x ** 2 - p.y ** 2
+    u2 = ps.solve_sipg_poisson_2d(p, 0 * uh, bc_types=osp.boundary_bc(o), u_dir=uh, iterative=cfg)
+    assert _rel_l2(p, u2, uh) < 1e-6
+
+
+@pytest.mark.parametrize("alpha", [1.0, 100.0])
+def test_helmholtz_cg_vs_lu(alpha):
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(8, 8, 3)
+    bc = osp.boundary_bc(o)
+    ue = np.sin(np.pi * p.x) * np.sin(np.pi * p.y)
+    f = (2 * np.pi ** 2 + alpha) * ue
+    u_lu = ps.solve_sipg_helmholtz_2d(p, f, alpha=alpha, nu=1.0, bc_types=bc)
+    u_cg = ps.solve_sipg_helmholtz_2d(p, f, alpha=alpha, nu=1.0, bc_types=bc,
+                                      iterative=ps.IterativeConfig(tol=1e-12, maxiter=2000))
+    assert _rel_l2(p, u_lu, ue) < 1e-3 and np.max(np.abs(u_cg - u_lu)) < 1e-8
+
+
+def test_singular_neumann_matches_oracle():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 6, 3)
+    bc = osp.boundary_bc(o, osp.BC_NEUMANN)
+    src = np.cos(np.pi * o.x) * np.cos(np.pi * o.y)
+    cfg = ps.IterativeConfig(tol=1e-12, maxiter=5000)
+    u_ref = osp.solve_poisson(o, src, bc_types=bc, iterative=osp.IterativeConfig(tol=1e-12, maxiter=5000))
+    u = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, iterative=cfg)
+    assert _rel(u, u_ref) < 1e-7
+    assert abs(u.sum()) < 1e-8 * np.abs(u).sum()
+
+
+def test_mixed_precision_refinement_reaches_fp64_accuracy():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(16, 16, 4)
+    bc = _bcs(o)["mixed"]
+    rng = np.random.default_rng(9)
+    src = rng.standard_normal((o.Np, o.K))
+    pc = ps.make_helmholtz_block_jacobi_preconditioner(p, alpha=5.0, nu=1.0, bc_types=bc)
+    u64 = ps.solve_sipg_helmholtz_2d(p, src, alpha=5.0, nu=1.0, bc_types=bc, preconditioner=pc,
+                                     iterative=ps.IterativeConfig(tol=1e-13, maxiter=10000))
+    um, info = ps.solve_sipg_helmholtz_2d(p, src, alpha=5.0, nu=1.0, bc_types=bc, preconditioner=pc,
+                                          iterative=ps.IterativeConfig(tol=1e-12, maxiter=10000,
+                                                                       precision="mixed"),
+                                          return_info=True)
+    assert info.status == "converged"
+    assert np.linalg.norm(um - u64) / np.linalg.norm(u64) < 1e-8
+
+
+def test_gmres_extension_matches_cg():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 6, 3)
+    bc = osp.boundary_bc(o)
+    src = np.random.default_rng(2).standard_normal((o.Np, o.K))
+    u_cg = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, tau_scale=0.5,
+                                    iterative=ps.IterativeConfig(tol=1e-11, maxiter=4000))
+    u_gm, info = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, return_info=True, tau_scale=0.5,
+                                          iterative=ps.IterativeConfig(method="gmres", tol=1e-11, maxiter=4000,
+                                                                       restart=60))
+    assert info.status == "converged" and _rel(u_gm, u_cg) < 1e-7
+
+
+def test_errors_are_raised():
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(2, 2, 2)
+    bc = osp.boundary_bc(o)
+    with pytest.raises(ValueError):
+        ps.solve_sipg_poisson_2d(p, 0 * p.x, bc_types=bc, iterative=ps.IterativeConfig(method="bicg"))
+    with pytest.raises(ValueError):
+        ps.sipg_apply_2d(p, 0 * p.x, bc_types=bc[:3])
+    with pytest.raises(ValueError):
+        ps.sipg_apply_2d(p, 0 * p.x, bc_types=bc, cub=object())
+
+
+# ------------------------- size-independent properties at full size
+
+def test_full_size_operator_symmetry_and_linearity():
+    """K = 131072, N = 4 (the precision workload's mesh): u.Av = v.Au and
+    A(au + bv) = aAu + bAv, float64, through the C ABI."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    m = pm.build_mesh_2d(*pm.uniform_rectangle_mesh_2d(0, 1, 0, 1, 256, 256), 4)
+    isb = m.EToE == np.arange(m.K)[:, None]
+    nx = m.nx.reshape((m.Nfp, 3, m.K), order="F")[0].T
+    bc = np.where(isb, np.where(np.abs(nx) > 0.5, 1, 2), 0).astype(np.int32)
+    op = m.device_operator(bc, 0.5)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    u = torch.randn(op.n, dtype=torch.float64, device="cuda", generator=g)
+    v = torch.randn(op.n, dtype=torch.float64, device="cuda", generator=g)
+    Au, Av = op.apply(u, alpha=5.0), op.apply(v, alpha=5.0)
+    s1, s2 = float(u @ Av), float(v @ Au)
+    assert abs(s1 - s2) <= 1e-12 * (abs(s1) + abs(s2))
+    w = op.apply(2.0 * u - 3.0 * v, alpha=5.0)
+    assert float(torch.max(torch.abs(w - (2.0 * Au - 3.0 * Av)))) <= 1e-12 * float(torch.max(torch.abs(w)))
+    assert float(u @ Au) > 0.0
