@@ -238,6 +238,23 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def profile_solves(args):
+    """One float64 and one mixed block-Jacobi PCG solve of the workload."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    m, bc, f = workload_arrays(pm.build_mesh_2d, pm.uniform_rectangle_mesh_2d)
+    pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE)
+    for prec in ("fp64", "mixed"):
+        cfg = ps.IterativeConfig(tol=args.solve_tol, maxiter=args.profile_maxiter, precision=prec,
+                                 inner_tol=args.inner_tol)
+        t0 = time.perf_counter()
+        _, info = ps.solve_sipg_helmholtz_2d(m, f, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE,
+                                             preconditioner=pc, iterative=cfg, return_info=True)
+        torch.cuda.synchronize()
+        print(prec, info, f"{time.perf_counter() - t0:.3f} s", flush=True)
+
+
 # ------------------------------------------------------------ CPU legs
 
 def cpu_baseline(budget_s=15.0):
@@ -275,16 +292,22 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--solve-tol", type=float, default=1e-12)
-    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--solve-tol", type=float, default=1e-10)
+    ap.add_argument("--inner-tol", type=float, default=0.1)
     ap.add_argument("--solve-reps", type=int, default=3)
     ap.add_argument("--skip-solves", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile-maxiter", type=int, default=20000)
+    ap.add_argument("--profile-solves", action="store_true",
+                    help="only the float64 and mixed solves, one each (for a profiler's launch list)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile_solves:
+        profile_solves(args)
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
         if line is not None:

@@ -18,7 +18,7 @@ DDG_FP32 = 1
 DDG_PC_NONE = 0
 DDG_PC_JACOBI = 1
 DDG_MAX_DEGREE = 5
-SOLVE_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "device_error"}
+SOLVE_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "device_error", 4: "stagnated"}
 
 
 class DdgError(RuntimeError):
@@ -49,7 +49,16 @@ class CgConfig(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("res_norm2", C.c_double),
-                ("b_norm2", C.c_double)]
+                ("b_norm2", C.c_double), ("updates", C.c_int32), ("reserved", C.c_int32)]
+
+
+class MgDesc(C.Structure):
+    _fields_ = [("nlevels", C.c_int32), ("precision", C.c_int32), ("nu", C.c_int32), ("reserved", C.c_int32),
+                ("omega", C.c_double), ("alpha", C.c_double),
+                ("ops", C.POINTER(C.c_void_p)),
+                ("prolong", C.POINTER(C.POINTER(C.c_double))),
+                ("prolong_rows", C.POINTER(C.c_int32)), ("prolong_cols", C.POINTER(C.c_int32)),
+                ("coarse_inv", C.POINTER(C.c_double))]
 
 
 _vp = C.c_void_p
@@ -64,6 +73,11 @@ _PROTOS = {
     "ddg_sipg_pc_apply": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "ddg_sipg_pc_blocks": (C.c_int, [_vp, _vp, _vp]),
     "ddg_sipg_cg": (C.c_int, [_vp, C.POINTER(CgConfig), _vp, _vp, _vp, C.POINTER(SolveInfo)]),
+    "ddg_sipg_cg_mixed": (C.c_int, [_vp, C.POINTER(CgConfig), C.c_double, _vp, _vp, _vp, C.POINTER(SolveInfo)]),
+    "ddg_mg_create": (C.c_int, [C.POINTER(MgDesc), C.POINTER(_vp)]),
+    "ddg_mg_destroy": (C.c_int, [_vp]),
+    "ddg_mg_apply": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ddg_sipg_cg_mg": (C.c_int, [_vp, C.POINTER(CgConfig), _vp, _vp, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_axpby": (C.c_int, [_i64, C.c_double, _vp, C.c_double, _vp, _vp]),
     "ddg_dot": (C.c_int, [_i64, C.c_int, _vp, _vp, _vp, _vp]),
     "ddg_cast": (C.c_int, [_i64, C.c_int, _vp, _vp, _vp]),

@@ -5,7 +5,9 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <algorithm>
 #include <cstring>
+#include <cstddef>
 #include <map>
 #include <mutex>
 #include <string>
@@ -84,6 +86,7 @@ struct ddg_sipg_op {
   CgCtl* ctl = nullptr;
   double* partA = nullptr;
   double* partB = nullptr;
+  double* partC = nullptr;
   unsigned int* ticket = nullptr;   // for the free dot helper
   double* dotbuf = nullptr;
   // block Jacobi
@@ -94,6 +97,7 @@ struct ddg_sipg_op {
   double pc_alpha = 0.0;
   Work w[2];
   std::map<GraphKey, CgGraph> graphs;
+  std::map<std::pair<void*, GraphKey>, CgGraph> mg_graphs;   // CG with a multigrid preconditioner
   cudaStream_t cap = nullptr;       // private stream for graph capture
   // host copies for set_bc
   std::vector<int64_t> EToE, EToF, vmapP;
@@ -203,6 +207,7 @@ int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGra
   c.ctl = op->ctl;
   c.partA = op->partA;
   c.partB = op->partB;
+  c.partC = op->partC;
   c.K = op->K;
   c.dev_status = op->status;
   c.has_cond = 1;
@@ -264,7 +269,11 @@ void free_op(ddg_sipg_op* op) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
   }
-  void* ptrs[] = {op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB,
+  for (auto& kv : op->mg_graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.g) cudaGraphDestroy(kv.second.g);
+  }
+  void* ptrs[] = {op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
                   op->ticket, op->dotbuf, op->blocks, op->binv64, op->binv32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -384,6 +393,7 @@ extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
   const int np_parts = std::max(apply_grid(K), std::max(cg_grid(K), dot_grid((int64_t)K * Np))) + 32;
   ALLOC(op->partA, np_parts * sizeof(double));
   ALLOC(op->partB, np_parts * sizeof(double));
+  ALLOC(op->partC, np_parts * sizeof(double));
   ALLOC(op->ticket, sizeof(unsigned int));
   ALLOC(op->dotbuf, sizeof(double));
 #undef ALLOC
@@ -474,8 +484,9 @@ extern "C" int ddg_sipg_pc_build(ddg_sipg_op* op, double alpha, void* stream) {
   const size_t nb = (size_t)op->K * op->Np * op->Np;
   if (!op->blocks) {
     CK(cudaMalloc((void**)&op->blocks, nb * 8));
-    CK(cudaMalloc((void**)&op->binv64, (size_t)op->Np * op->Np * op->ldb * 8));
-    CK(cudaMalloc((void**)&op->binv32, (size_t)op->Np * op->Np * op->ldb * 4));
+    const size_t nsym = (size_t)op->Np * (op->Np + 1) / 2;
+    CK(cudaMalloc((void**)&op->binv64, nsym * op->ldb * 8));
+    CK(cudaMalloc((void**)&op->binv32, nsym * op->ldb * 4));
   }
   BlockArgs a{};
   a.geo = op->geo64;
@@ -573,6 +584,7 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
     c.ctl = op->ctl;
     c.partA = op->partA;
     c.partB = op->partB;
+    c.partC = op->partC;
     c.K = op->K;
     c.dev_status = op->status;
     if (e == cudaSuccess) e = launch_cg_step<double>(op->N, cfg->pc != 0, true, c, s);
@@ -594,6 +606,7 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
     c.ctl = op->ctl;
     c.partA = op->partA;
     c.partB = op->partB;
+    c.partC = op->partC;
     c.K = op->K;
     c.dev_status = op->status;
     if (e == cudaSuccess) e = launch_cg_step<float>(op->N, cfg->pc != 0, true, c, s);
@@ -662,5 +675,487 @@ extern "C" int ddg_dot(int64_t n, int prec, const void* x, const void* y, double
   }
   cudaError_t e = launch_dot(n, prec, x, y, sc.first, sc.second, out, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("dot: ") + cudaGetErrorString(e));
+  return DDG_OK;
+}
+
+extern "C" int ddg_sipg_cg_mixed(ddg_sipg_op* op, const ddg_cg_config* cfg, double delta, const double* b,
+                                 double* x, void* stream, ddg_solve_info* info) {
+  if (!op || !cfg || !b || !x) return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mixed: null argument");
+  if (cfg->maxiter < 0 || !(cfg->tol >= 0) || !(cfg->atol >= 0) || !(delta > 0.0 && delta < 1.0))
+    return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mixed: need tol, atol, maxiter >= 0 and 0 < delta < 1");
+  if (cfg->pc != DDG_PC_NONE && cfg->pc != DDG_PC_JACOBI) return fail(DDG_ERR_UNSUPPORTED, "ddg_sipg_cg_mixed: pc kind");
+  if (cfg->pc == DDG_PC_JACOBI && (!op->pc_ready || op->pc_alpha != cfg->alpha))
+    return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mixed: block-Jacobi preconditioner missing or built for another alpha");
+  DevGuard guard(op->dev);
+  int rc = ensure_work(op, DDG_FP64);
+  if (rc == DDG_OK) rc = ensure_work(op, DDG_FP32);
+  if (rc != DDG_OK) return rc;
+  Work& w64 = op->w[DDG_FP64];
+  Work& w32 = op->w[DDG_FP32];
+  GraphKey key{DDG_FP32, cfg->pc, cfg->alpha, cfg->shift};
+  CgGraph* gr = nullptr;
+  rc = get_graph(op, key, &gr);
+  if (rc != DDG_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = (int64_t)op->K * op->Np;
+  CK(cudaMemcpyAsync(w64.b, b, w64.bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(w64.x, x, w64.bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemsetAsync(op->ctl, 0, sizeof(CgCtl), s));
+
+  ApplyArgs<double> ra = apply_args<double>(op);
+  ra.in0 = (const double*)w64.x;
+  ra.in1 = (const double*)w64.b;
+  ra.out0 = (double*)w64.r;
+  ra.alpha = cfg->alpha;
+  ra.shift = cfg->shift;
+  ra.use_tma = 1;
+  CgArgs<float> ci{};
+  ci.r = (float*)w32.r;
+  ci.z = cfg->pc ? (float*)w32.z : (float*)w32.r;
+  ci.p_zero = (float*)w32.p0;
+  ci.binv = op->binv32;
+  ci.ldb = op->ldb;
+  ci.ctl = op->ctl;
+  ci.partA = op->partA;
+  ci.partB = op->partB;
+  ci.partC = op->partC;
+  ci.dev_status = op->status;
+  ci.K = op->K;
+
+  double target = -1.0;
+  std::vector<double> hist;
+  int total = 0, updates = 0, status = DDG_SOLVE_MAXITER;
+  double rr_last = 0.0, bb0 = 0.0;
+  for (int outer = 0; outer < 100000; ++outer) {
+    // float64 true residual r = b - (alpha M + A + shift) x
+    cudaError_t e = launch_apply<double>(op->N, AM_RESID, ra, s);
+    if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("residual launch: ") + cudaGetErrorString(e));
+    CgCtl h{};
+    CK(cudaMemcpyAsync(&h, op->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (target < 0.0) {
+      bb0 = h.bb;
+      target = std::fmax(cfg->tol * cfg->tol * h.bb, cfg->atol * cfg->atol);
+    }
+    rr_last = h.rr;
+    hist.push_back(h.rr);
+    if (!std::isfinite(h.rr)) {
+      status = DDG_SOLVE_BREAKDOWN;
+      break;
+    }
+    if (h.rr <= target) {
+      status = DDG_SOLVE_CONVERGED;
+      break;
+    }
+    if (total >= cfg->maxiter) {
+      status = DDG_SOLVE_MAXITER;
+      break;
+    }
+    const size_t m = hist.size();
+    if (m >= 4 && hist[m - 1] > 0.5 * hist[m - 2] && hist[m - 2] > 0.5 * hist[m - 3] &&
+        hist[m - 3] > 0.5 * hist[m - 4]) {
+      status = DDG_SOLVE_STAGNATED;
+      break;
+    }
+    // float32 restart from the float64 residual, keeping the direction
+    struct {
+      double tol2, atol_sq;
+    } tl{delta * delta, 0.0};
+    struct {
+      int iter, maxiter, status, use_pc, cont;
+    } it{0, cfg->maxiter - total, 0, cfg->pc != DDG_PC_NONE, 1};
+    CK(cudaMemcpyAsync((char*)op->ctl + offsetof(CgCtl, tol2), &tl, sizeof(tl), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync((char*)op->ctl + offsetof(CgCtl, iter), &it, sizeof(it), cudaMemcpyHostToDevice, s));
+    e = launch_cast_norm(n, (const double*)w64.r, (float*)w32.r, (float*)w32.x, op->partA, op->ctl, s);
+    ci.keep_p = updates > 0 ? 1 : 0;
+    if (e == cudaSuccess) e = launch_cg_step<float>(op->N, cfg->pc != 0, true, ci, s);
+    if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("mixed restart launch: ") + cudaGetErrorString(e));
+    CK(cudaGraphLaunch(gr->exec, s));
+    CgCtl h2{};
+    CK(cudaMemcpyAsync(&h2, op->ctl, sizeof(h2), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    total += h2.iter;
+    // the ping-pong body leaves the newest direction in p1 after an odd count
+    if (h2.iter % 2 == 1) CK(cudaMemcpyAsync(w32.p0, w32.p1, w32.bytes, cudaMemcpyDeviceToDevice, s));
+    e = launch_axpy_mixed(n, (const float*)w32.x, (double*)w64.x, s);
+    if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("mixed update launch: ") + cudaGetErrorString(e));
+    ++updates;
+    if (h2.status == 2 || h2.status == 3) {
+      status = h2.status == 3 ? DDG_SOLVE_DEVICE_ERR : DDG_SOLVE_BREAKDOWN;
+      break;
+    }
+    if (h2.iter == 0) {
+      status = DDG_SOLVE_STAGNATED;
+      break;
+    }
+  }
+  CK(cudaMemcpyAsync(x, w64.x, w64.bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  rc = check_status(op);
+  if (rc != DDG_OK) return rc;
+  if (info) {
+    info->status = status;
+    info->iterations = total;
+    info->res_norm2 = rr_last;
+    info->b_norm2 = bb0;
+    info->updates = updates;
+  }
+  return DDG_OK;
+}
+
+// =========================================================== multigrid
+struct ddg_mg {
+  int L = 0, prec = 1, nu = 2, dev = 0;
+  double omega = 0.7, alpha = 0.0;
+  std::vector<ddg_sipg_op*> ops;
+  struct Lv {
+    int n = 0, Kc = 0, prow = 0, pcol = 0;   // Kc: K of the next coarser level
+    void *x = nullptr, *t = nullptr, *b = nullptr, *r = nullptr;
+    void *P = nullptr, *R = nullptr;          // prolongation / restriction (MG precision)
+  };
+  std::vector<Lv> lv;
+  void* Ainv = nullptr;
+  int nc = 0;
+  CgCtl* sctl = nullptr;                     // scratch control block for residual kernels
+  double *spa = nullptr, *spb = nullptr;
+  std::vector<ddg_sipg_op*> users;           // handles holding CG graphs that embed this V-cycle
+};
+
+namespace {
+
+template <typename T>
+int mg_alloc(ddg_mg* mg, const ddg_mg_desc* d) {
+  const size_t ts = sizeof(T);
+  int maxK = 0;
+  for (int l = 0; l < mg->L; ++l) maxK = std::max(maxK, mg->ops[l]->K);
+  cudaError_t e = cudaSuccess;
+  for (int l = 0; l < mg->L; ++l) {
+    auto& v = mg->lv[l];
+    v.n = mg->ops[l]->K * mg->ops[l]->Np;
+    void** bufs[] = {&v.x, &v.t, &v.b, &v.r};
+    for (void** p : bufs)
+      if (e == cudaSuccess) e = cudaMalloc(p, (size_t)v.n * ts);
+    if (l + 1 < mg->L) {
+      const int rows = d->prolong_rows[l], cols = d->prolong_cols[l];
+      std::vector<T> P((size_t)rows * cols), R((size_t)rows * cols);
+      for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < cols; ++j) {
+          P[(size_t)i * cols + j] = (T)d->prolong[l][(size_t)i * cols + j];
+          R[(size_t)j * rows + i] = (T)d->prolong[l][(size_t)i * cols + j];
+        }
+      v.prow = rows;
+      v.pcol = cols;
+      v.Kc = mg->ops[l + 1]->K;
+      if (e == cudaSuccess) e = cudaMalloc(&v.P, P.size() * ts);
+      if (e == cudaSuccess) e = cudaMalloc(&v.R, R.size() * ts);
+      if (e == cudaSuccess) e = cudaMemcpy(v.P, P.data(), P.size() * ts, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(v.R, R.data(), R.size() * ts, cudaMemcpyHostToDevice);
+    }
+  }
+  const int nc = mg->lv[mg->L - 1].n;
+  mg->nc = nc;
+  std::vector<T> A((size_t)nc * nc);
+  for (size_t i = 0; i < A.size(); ++i) A[i] = (T)d->coarse_inv[i];
+  if (e == cudaSuccess) e = cudaMalloc(&mg->Ainv, A.size() * ts);
+  if (e == cudaSuccess) e = cudaMemcpy(mg->Ainv, A.data(), A.size() * ts, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&mg->sctl, sizeof(CgCtl));
+  if (e == cudaSuccess) e = cudaMemset(mg->sctl, 0, sizeof(CgCtl));
+  const int np = apply_grid(maxK) + 32;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&mg->spa, np * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&mg->spb, np * sizeof(double));
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? DDG_ERR_NOMEM : DDG_ERR_CUDA,
+                std::string("ddg_mg_create: ") + cudaGetErrorString(e));
+  return DDG_OK;
+}
+
+void mg_free(ddg_mg* mg) {
+  for (auto& v : mg->lv) {
+    void* p[] = {v.x, v.t, v.b, v.r, v.P, v.R};
+    for (void* q : p)
+      if (q) cudaFree(q);
+  }
+  void* p[] = {mg->Ainv, mg->sctl, mg->spa, mg->spb};
+  for (void* q : p)
+    if (q) cudaFree(q);
+  delete mg;
+}
+
+template <typename T>
+ApplyArgs<T> mg_args(ddg_mg* mg, int l) {
+  ApplyArgs<T> a = apply_args<T>(mg->ops[l]);
+  a.ctl = mg->sctl;
+  a.partA = mg->spa;
+  a.partB = mg->spb;
+  a.alpha = mg->alpha;
+  a.use_tma = 1;
+  a.binv = (sizeof(T) == 8) ? (const T*)mg->ops[l]->binv64 : (const T*)mg->ops[l]->binv32;
+  a.ldb = mg->ops[l]->ldb;
+  a.omega = mg->omega;
+  return a;
+}
+
+// One V-cycle on level l: approximately solves A_l x = b_l (b_l in lv[l].b).
+// Returns the buffer that holds x_l.  Only kernel launches: capturable.
+template <typename T>
+cudaError_t mg_vcycle(ddg_mg* mg, int l, cudaStream_t s, T** result) {
+  auto& v = mg->lv[l];
+  ddg_sipg_op* op = mg->ops[l];
+  cudaError_t e;
+  if (l == mg->L - 1) {   // coarse: x = A_c^-1 b (multigrid.py:227-228)
+    e = launch_dense_gemv<T>(mg->nc, (const T*)mg->Ainv, (const T*)v.b, (T*)v.x, s);
+    *result = (T*)v.x;
+    return e;
+  }
+  T* A = (T*)v.x;
+  T* B = (T*)v.t;
+  const T* binv = (sizeof(T) == 8) ? (const T*)op->binv64 : (const T*)op->binv32;
+  ApplyArgs<T> a = mg_args<T>(mg, l);
+  // pre-smoothing from x = 0: the first sweep is x = omega B^-1 b
+  if (mg->nu > 0) {
+    e = launch_bj_scaled<T>(op->N, (const T*)v.b, A, binv, op->ldb, op->K, (T)mg->omega, s);
+    if (e != cudaSuccess) return e;
+  } else {
+    e = cudaMemsetAsync(A, 0, (size_t)v.n * sizeof(T), s);
+    if (e != cudaSuccess) return e;
+  }
+  for (int it = 1; it < mg->nu; ++it) {
+    a.in0 = A; a.in1 = (const T*)v.b; a.out0 = B;
+    if ((e = launch_apply<T>(op->N, AM_SMOOTH, a, s)) != cudaSuccess) return e;
+    std::swap(A, B);
+  }
+  // coarse-grid correction
+  a.in0 = A; a.in1 = (const T*)v.b; a.out0 = (T*)v.r;
+  if ((e = launch_apply<T>(op->N, AM_RESID, a, s)) != cudaSuccess) return e;
+  auto& c = mg->lv[l + 1];
+  if ((e = launch_elem_matvec<T>(v.Kc, v.pcol, v.prow, (const T*)v.R, (const T*)v.r, (T*)c.b, 0, s)) != cudaSuccess)
+    return e;
+  T* xc = nullptr;
+  if ((e = mg_vcycle<T>(mg, l + 1, s, &xc)) != cudaSuccess) return e;
+  if ((e = launch_elem_matvec<T>(v.Kc, v.prow, v.pcol, (const T*)v.P, xc, A, 1, s)) != cudaSuccess) return e;
+  for (int it = 0; it < mg->nu; ++it) {
+    a.in0 = A; a.in1 = (const T*)v.b; a.out0 = B;
+    if ((e = launch_apply<T>(op->N, AM_SMOOTH, a, s)) != cudaSuccess) return e;
+    std::swap(A, B);
+  }
+  *result = A;
+  return cudaSuccess;
+}
+
+// every smoothed level must still carry the smoother built for mg->alpha
+int mg_check(ddg_mg* mg) {
+  for (int l = 0; l + 1 < mg->L; ++l)
+    if (!mg->ops[l]->pc_ready || mg->ops[l]->pc_alpha != mg->alpha)
+      return fail(DDG_ERR_INVALID, "multigrid level " + std::to_string(l) +
+                                       ": its block-Jacobi smoother was rebuilt for another alpha");
+  return DDG_OK;
+}
+
+// z = V(r) with float64 r, z (casts around a float32 hierarchy)
+cudaError_t mg_apply64(ddg_mg* mg, const double* r, double* z, cudaStream_t s) {
+  const int64_t n = mg->lv[0].n;
+  cudaError_t e;
+  if (mg->prec == DDG_FP32) {
+    if ((e = launch_cast(n, DDG_FP32, r, mg->lv[0].b, s)) != cudaSuccess) return e;
+    float* res = nullptr;
+    if ((e = mg_vcycle<float>(mg, 0, s, &res)) != cudaSuccess) return e;
+    return launch_cast(n, DDG_FP64, res, z, s);
+  }
+  if ((e = cudaMemcpyAsync(mg->lv[0].b, r, n * 8, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+  double* res = nullptr;
+  if ((e = mg_vcycle<double>(mg, 0, s, &res)) != cudaSuccess) return e;
+  return cudaMemcpyAsync(z, res, n * 8, cudaMemcpyDeviceToDevice, s);
+}
+
+int get_mg_graph(ddg_sipg_op* op, ddg_mg* mg, const GraphKey& key, CgGraph** out) {
+  auto k2 = std::make_pair((void*)mg, key);
+  auto it = op->mg_graphs.find(k2);
+  if (it != op->mg_graphs.end()) {
+    *out = &it->second;
+    return DDG_OK;
+  }
+  Work& w = op->w[DDG_FP64];
+  const int64_t n = (int64_t)op->K * op->Np;
+  CgGraph cg;
+  CK(cudaGraphCreate(&cg.g, 0));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, cg.g, 1, cudaGraphCondAssignDefault));
+  alignas(cudaGraphNodeParams) unsigned char np_buf[sizeof(cudaGraphNodeParams)];
+  std::memset(np_buf, 0, sizeof(np_buf));
+  cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_buf);
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, cg.g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(op->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  ApplyArgs<double> a = apply_args<double>(op);
+  a.alpha = key.alpha;
+  a.shift = key.shift;
+  a.use_tma = 1;
+  cudaError_t e = cudaSuccess;
+  for (int half = 0; half < 2 && e == cudaSuccess; ++half) {
+    void* pin = half == 0 ? w.p0 : w.p1;
+    void* pout = half == 0 ? w.p1 : w.p0;
+    a.in0 = (const double*)w.z;
+    a.in1 = (const double*)pin;
+    a.out0 = (double*)w.Ap;
+    a.out1 = (double*)pout;
+    e = launch_apply<double>(op->N, AM_PFUSE, a, op->cap);
+    if (e == cudaSuccess)
+      e = launch_cg_xr<double>((double*)w.x, (const double*)pout, (double*)w.r, (const double*)w.Ap, n, op->ctl,
+                               op->partA, op->cap);
+    if (e == cudaSuccess) e = mg_apply64(mg, (const double*)w.r, (double*)w.z, op->cap);
+    if (e == cudaSuccess)
+      e = launch_cg_finish<double>(false, (const double*)w.r, (const double*)w.z, n, op->ctl, op->partA,
+                                   op->status, 1, h, op->cap);
+  }
+  cudaGraph_t outg = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(op->cap, &outg);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    cudaGraphDestroy(cg.g);
+    return fail(DDG_ERR_CUDA, std::string("MG-CG body capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  CK(cudaGraphInstantiate(&cg.exec, cg.g, 0));
+  op->mg_graphs[k2] = cg;
+  *out = &op->mg_graphs[k2];
+  if (std::find(mg->users.begin(), mg->users.end(), op) == mg->users.end()) mg->users.push_back(op);
+  return DDG_OK;
+}
+
+}  // namespace
+
+extern "C" int ddg_mg_create(const ddg_mg_desc* d, ddg_mg** out) {
+  if (!d || !out || d->nlevels < 1 || !d->ops || !d->coarse_inv)
+    return fail(DDG_ERR_INVALID, "ddg_mg_create: bad descriptor");
+  if (d->precision != DDG_FP32 && d->precision != DDG_FP64) return fail(DDG_ERR_INVALID, "ddg_mg_create: precision");
+  if (d->nu < 0 || !(d->omega > 0.0)) return fail(DDG_ERR_INVALID, "ddg_mg_create: nu >= 0, omega > 0");
+  *out = nullptr;
+  for (int l = 0; l < d->nlevels; ++l) {
+    ddg_sipg_op* op = d->ops[l];
+    if (!op) return fail(DDG_ERR_INVALID, "ddg_mg_create: null level handle");
+    if (l + 1 < d->nlevels && (!op->pc_ready || op->pc_alpha != d->alpha))
+      return fail(DDG_ERR_INVALID, "ddg_mg_create: level " + std::to_string(l) +
+                                       " needs ddg_sipg_pc_build(alpha) for its smoother");
+    if (op->dev != d->ops[0]->dev) return fail(DDG_ERR_INVALID, "ddg_mg_create: levels on different devices");
+  }
+  for (int l = 0; l + 1 < d->nlevels; ++l) {
+    ddg_sipg_op *f = d->ops[l], *c = d->ops[l + 1];
+    const int rows = d->prolong_rows[l], cols = d->prolong_cols[l];
+    const bool pt = (f->K == c->K) && rows == f->Np && cols == c->Np;
+    const bool ht = (f->K == 4 * c->K) && f->Np == c->Np && rows == 4 * f->Np && cols == c->Np;
+    if (!pt && !ht || !d->prolong[l])
+      return fail(DDG_ERR_INVALID, "ddg_mg_create: transfer " + std::to_string(l) +
+                                       " is neither a p-transfer (same K) nor an h-transfer (K = 4 Kc)");
+  }
+  const int Lc = d->nlevels - 1;
+  const int64_t nc = (int64_t)d->ops[Lc]->K * d->ops[Lc]->Np;
+  if (nc > 20000) return fail(DDG_ERR_INVALID, "ddg_mg_create: coarsest level too large for a dense solve");
+  DevGuard guard(d->ops[0]->dev);
+  ddg_mg* mg = new ddg_mg();
+  mg->L = d->nlevels;
+  mg->prec = d->precision;
+  mg->nu = d->nu;
+  mg->omega = d->omega;
+  mg->alpha = d->alpha;
+  mg->dev = d->ops[0]->dev;
+  mg->ops.assign(d->ops, d->ops + d->nlevels);
+  mg->lv.resize(d->nlevels);
+  const int rc = d->precision == DDG_FP32 ? mg_alloc<float>(mg, d) : mg_alloc<double>(mg, d);
+  if (rc != DDG_OK) {
+    mg_free(mg);
+    return rc;
+  }
+  *out = mg;
+  return DDG_OK;
+}
+
+extern "C" int ddg_mg_destroy(ddg_mg* mg) {
+  if (!mg) return DDG_OK;
+  DevGuard guard(mg->dev);
+  cudaDeviceSynchronize();
+  for (ddg_sipg_op* op : mg->users) {     // drop CG graphs that embed this V-cycle
+    for (auto it = op->mg_graphs.begin(); it != op->mg_graphs.end();) {
+      if (it->first.first == (void*)mg) {
+        if (it->second.exec) cudaGraphExecDestroy(it->second.exec);
+        if (it->second.g) cudaGraphDestroy(it->second.g);
+        it = op->mg_graphs.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  mg_free(mg);
+  return DDG_OK;
+}
+
+extern "C" int ddg_mg_apply(ddg_mg* mg, const double* r, double* z, void* stream) {
+  if (!mg || !r || !z) return fail(DDG_ERR_INVALID, "ddg_mg_apply: null argument");
+  if (int rc = mg_check(mg)) return rc;
+  DevGuard guard(mg->dev);
+  cudaError_t e = mg_apply64(mg, r, z, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("ddg_mg_apply: ") + cudaGetErrorString(e));
+  return DDG_OK;
+}
+
+extern "C" int ddg_sipg_cg_mg(ddg_sipg_op* op, const ddg_cg_config* cfg, ddg_mg* mg, const double* b, double* x,
+                              void* stream, ddg_solve_info* info) {
+  if (!op || !cfg || !mg || !b || !x) return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mg: null argument");
+  if (cfg->maxiter < 0 || !(cfg->tol >= 0) || !(cfg->atol >= 0))
+    return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mg: tol/atol/maxiter must be non-negative");
+  if (mg->lv[0].n != op->K * op->Np || mg->ops[0]->N != op->N)
+    return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mg: finest multigrid level does not match the operator");
+  if (mg->dev != op->dev) return fail(DDG_ERR_INVALID, "ddg_sipg_cg_mg: different devices");
+  if (int rc0 = mg_check(mg)) return rc0;
+  DevGuard guard(op->dev);
+  int rc = ensure_work(op, DDG_FP64);
+  if (rc != DDG_OK) return rc;
+  Work& w = op->w[DDG_FP64];
+  cudaStream_t s = (cudaStream_t)stream;
+  GraphKey key{DDG_FP64, 99, cfg->alpha, cfg->shift};
+  CgGraph* gr = nullptr;
+  rc = get_mg_graph(op, mg, key, &gr);
+  if (rc != DDG_OK) return rc;
+  const int64_t n = (int64_t)op->K * op->Np;
+  CgCtl h{};
+  h.tol2 = cfg->tol * cfg->tol;
+  h.atol_sq = cfg->atol * cfg->atol;
+  h.maxiter = cfg->maxiter;
+  h.use_pc = 1;
+  h.cont = 1;
+  h.zcoef = 1.0;
+  CK(cudaMemcpyAsync(op->ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(w.b, b, w.bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(w.x, x, w.bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemsetAsync(w.p0, 0, w.bytes, s));
+  ApplyArgs<double> a = apply_args<double>(op);
+  a.in0 = (const double*)w.x;
+  a.in1 = (const double*)w.b;
+  a.out0 = (double*)w.r;
+  a.alpha = cfg->alpha;
+  a.shift = cfg->shift;
+  a.use_tma = 1;
+  cudaError_t e = launch_apply<double>(op->N, AM_RESID, a, s);
+  if (e == cudaSuccess) e = mg_apply64(mg, (const double*)w.r, (double*)w.z, s);
+  if (e == cudaSuccess)
+    e = launch_cg_finish<double>(true, (const double*)w.r, (const double*)w.z, n, op->ctl, op->partA, op->status, 0,
+                                 0, s);
+  if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("MG-CG init: ") + cudaGetErrorString(e));
+  CK(cudaGraphLaunch(gr->exec, s));
+  CK(cudaMemcpyAsync(x, w.x, w.bytes, cudaMemcpyDeviceToDevice, s));
+  CgCtl res{};
+  CK(cudaMemcpyAsync(&res, op->ctl, sizeof(res), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  rc = check_status(op);
+  if (rc != DDG_OK) return rc;
+  if (info) {
+    info->status = res.status;
+    info->iterations = res.iter;
+    info->res_norm2 = res.rr;
+    info->b_norm2 = res.bb;
+    info->updates = 0;
+  }
   return DDG_OK;
 }

@@ -58,6 +58,12 @@ struct RefMats {
 // specialises CRef for every built degree.
 template <int N, typename T> struct CRef;
 
+// Symmetric packed index of (i, j), upper triangle (block-Jacobi inverses
+// are stored as Np (Np + 1) / 2 entries per element).
+__host__ __device__ constexpr int sym_idx(int Np, int i, int j) {
+  return i <= j ? i * Np - i * (i - 1) / 2 + (j - i) : j * Np - j * (j - 1) / 2 + (i - j);
+}
+
 // ---------------------------------------------------------------- layout
 // Geometry: structure-of-arrays geo[c * ldg + k].
 enum GeoField { G_RX = 0, G_SX, G_RY, G_SY, G_J, G_F0 = 5, G_COUNT = 14 };
@@ -181,6 +187,7 @@ __device__ __forceinline__ void reduce_partials2(const double* pa, const double*
 // --------------------------------------------------- CG control block
 struct CgCtl {
   double gamma;   // r.z
+  double gamma_prev;  // r.z one iteration earlier (reliable-update restarts)
   double pAp;
   double alpha;
   double beta;
@@ -188,6 +195,7 @@ struct CgCtl {
   double bb;      // b.b
   double atol2;   // max(tol^2 b.b, atol^2)
   double tol2, atol_sq;
+  double zcoef;   // next direction p = zcoef z + beta p (1 except right after a restart)
   int iter, maxiter, status, use_pc;
   int cont;       // loop condition mirror (1 = keep iterating)
   unsigned int ticket;
@@ -231,17 +239,17 @@ struct NbrPlain {  // u~[i] = u[k' Np + perm[f'][i]]
   }
 };
 template <typename T, int Np>
-struct NbrPfuse {  // u~ = z~ + beta p_old~  (the CG direction update, fused)
+struct NbrPfuse {  // u~ = zc z~ + beta p_old~  (the CG direction update, fused)
   const T* __restrict__ z;
   const T* __restrict__ p;
-  T beta;
+  T zc, beta;
   const int* perm;
   __device__ __forceinline__ void operator()(int kp, int fp, T (&ut)[Np]) const {
     const size_t o = (size_t)kp * Np;
 #pragma unroll
     for (int i = 0; i < Np; ++i) {
       const int j = perm[fp * Np + i];
-      ut[i] = __ldg(z + o + j) + beta * __ldg(p + o + j);
+      ut[i] = zc * __ldg(z + o + j) + beta * __ldg(p + o + j);
     }
   }
 };

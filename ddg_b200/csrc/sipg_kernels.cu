@@ -39,10 +39,13 @@ DDG_CREF(5)
 //                 ctl->alpha = gamma / pAp  (last block)
 //       AM_RESID  out0 = in1 - (A in0 + ...); partials in1.in1, out0.out0
 //                 -> ctl->bb, ctl->rr (last block)
+//       AM_SMOOTH out0 = in0 + omega B^-1 (in1 - (A in0 + ...)): one weighted
+//                 block-Jacobi sweep (multigrid.py:238-243); out0 != in0
 template <int N, typename T, int MODE, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
   constexpr int Np = Dim<N>::Np;
   constexpr int NT = (MODE == AM_APPLY) ? 1 : 2;
+  constexpr bool HASB = (MODE == AM_RESID || MODE == AM_SMOOTH);
   __shared__ __align__(128) T s_tile[NT][BLOCK * Np];
   __shared__ int s_perm[3 * Np];
   __shared__ __align__(8) uint64_t s_bar;
@@ -81,6 +84,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
   }
 
   const T beta = (MODE == AM_PFUSE) ? T(a.ctl->beta) : T(0);
+  const T zc = (MODE == AM_PFUSE) ? T(a.ctl->zcoef) : T(1);
   const int k = k0 + tid;
   const bool active = tid < nk;
   T u[Np], y[Np], b2[Np];
@@ -89,18 +93,18 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
 #pragma unroll
     for (int i = 0; i < Np; ++i) {
       if (MODE == AM_PFUSE) {
-        u[i] = s_tile[0][tid * Np + i] + beta * s_tile[1][tid * Np + i];
+        u[i] = zc * s_tile[0][tid * Np + i] + beta * s_tile[1][tid * Np + i];
       } else {
         u[i] = s_tile[0][tid * Np + i];
       }
-      if (MODE == AM_RESID) b2[i] = s_tile[1][tid * Np + i];
+      if (HASB) b2[i] = s_tile[1][tid * Np + i];
     }
     uint32_t w[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
     const Geo<T> g = load_geo(a.geo, a.ldg, k);
     if (MODE == AM_PFUSE) {
-      NbrPfuse<T, Np> src{a.in0, a.in1, beta, s_perm};
+      NbrPfuse<T, Np> src{a.in0, a.in1, zc, beta, s_perm};
       elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src);
     } else {
       NbrPlain<T, Np> src{a.in0, s_perm};
@@ -110,7 +114,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
 #pragma unroll
       for (int i = 0; i < Np; ++i) y[i] += T(a.shift) * u[i];
     }
-    if (MODE == AM_RESID) {
+    if (HASB) {
 #pragma unroll
       for (int i = 0; i < Np; ++i) {
         y[i] = b2[i] - y[i];
@@ -124,7 +128,24 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
     }
   }
   __syncthreads();  // every tile read done before the tiles are overwritten
-  if (active) {
+  if (MODE == AM_SMOOTH) {
+    // residual of each element into tile 1, then x += omega B^-1 r with one
+    // (element, row) pair per thread (coalesced packed-inverse loads)
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < Np; ++i) s_tile[1][tid * Np + i] = y[i];
+    }
+    __syncthreads();
+    const T om = T(a.omega);
+    for (int idx = tid; idx < nk * Np; idx += BLOCK) {
+      const int i = idx / nk, e = idx - i * nk;
+      const T* rv = s_tile[1] + e * Np;
+      T acc = T(0);
+#pragma unroll
+      for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.ldb + k0 + e), rv[j], acc);
+      s_tile[0][e * Np + i] += om * acc;
+    }
+  } else if (active) {
 #pragma unroll
     for (int i = 0; i < Np; ++i) {
       s_tile[0][tid * Np + i] = y[i];
@@ -146,7 +167,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
       if (MODE == AM_PFUSE) a.out1[off + i] = s_tile[1][i];
     }
   }
-  if (MODE == AM_APPLY) return;
+  if (MODE == AM_APPLY || MODE == AM_SMOOTH) return;
 
   // reductions: block partials -> last block -> control block
   block_sum2<BLOCK>(dA, dB, s_red);
@@ -185,6 +206,7 @@ template <int N, typename T, bool PC, bool INIT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
   constexpr int Np = Dim<N>::Np;
   __shared__ __align__(16) T s_r[BLOCK * Np];
+  __shared__ __align__(16) T s_z[PC ? BLOCK * Np : 1];
   __shared__ double s_red[64];
   if (!INIT && a.ctl->cont == 0) {
     // the loop already stopped: make sure the while node sees 0
@@ -196,12 +218,13 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
   const int nk = min(BLOCK, a.K - k0);
   const size_t off = (size_t)k0 * Np;
   const T al = INIT ? T(0) : T(a.ctl->alpha);
-  double rr = 0.0, rz = 0.0;
+  double rr = 0.0, rz = 0.0, rp = 0.0;
   for (int i = tid; i < nk * Np; i += BLOCK) {
     T rn;
     if (INIT) {
       rn = a.r[off + i];
-      a.p_zero[off + i] = T(0);
+      if (!a.keep_p) a.p_zero[off + i] = T(0);
+      else rp += (double)rn * (double)a.p_zero[off + i];
     } else {
       a.x[off + i] += al * a.p[off + i];
       rn = a.r[off + i] - al * a.Ap[off + i];
@@ -211,45 +234,53 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
     if (PC) s_r[i] = rn;
   }
   if (PC) {
+    // z = B^-1 r, one (element, row) pair per thread: loads of the packed
+    // inverse are coalesced across the elements of a warp
     __syncthreads();
-    if (tid < nk) {
-      const int k = k0 + tid;
-      T rv[Np], zv[Np];
+    for (int idx = tid; idx < nk * Np; idx += BLOCK) {
+      const int i = idx / nk, e = idx - i * nk;
+      const T* rv = s_r + e * Np;
+      T acc = T(0);
 #pragma unroll
-      for (int j = 0; j < Np; ++j) rv[j] = s_r[tid * Np + j];
-#pragma unroll
-      for (int i = 0; i < Np; ++i) {
-        T acc = T(0);
-#pragma unroll
-        for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)(i * Np + j) * a.ldb + k), rv[j], acc);
-        zv[i] = acc;
-        rz += (double)rv[i] * (double)acc;
-      }
-#pragma unroll
-      for (int i = 0; i < Np; ++i) s_r[tid * Np + i] = zv[i];
+      for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.ldb + k0 + e), rv[j], acc);
+      s_z[e * Np + i] = acc;
+      rz += (double)rv[i] * (double)acc;
     }
     __syncthreads();
-    for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_r[i];
+    for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_z[i];
   } else {
     rz = rr;
   }
   block_sum2<BLOCK>(rz, rr, s_red);
+  if (INIT) {
+    double d0 = 0.0;
+    block_sum2<BLOCK>(rp, d0, s_red);
+  }
   if (tid == 0) {
     a.partA[blockIdx.x] = rz;
     a.partB[blockIdx.x] = rr;
+    if (INIT) a.partC[blockIdx.x] = rp;
   }
   if (!is_last_block(&a.ctl->ticket)) return;
-  double g, r2;
+  double g, r2, gp = 0.0, d1;
   reduce_partials2<BLOCK>(a.partA, a.partB, gridDim.x, g, r2, s_red);
+  if (INIT && a.keep_p) reduce_partials2<BLOCK>(a.partC, nullptr, gridDim.x, gp, d1, s_red);
   if (tid == 0) {
     CgCtl* c = a.ctl;
     if (INIT) {
       c->atol2 = fmax(c->tol2 * c->bb, c->atol_sq);
-      c->beta = 0.0;
+      // a reliable-update restart keeps the search direction: beta from the
+      // previous gamma; a fresh start has p_old = 0 and beta = 0
+      c->beta = (a.keep_p && c->gamma_prev != 0.0) ? g / c->gamma_prev : 0.0;
+      // restore r.p = 0 after the residual replacement:
+      // p_old <- p_old - (r.p_old / r.z) z, folded into the next direction
+      c->zcoef = (a.keep_p && g != 0.0) ? 1.0 - c->beta * (gp / g) : 1.0;
       c->iter = 0;
       c->status = 0;
     } else {
+      c->gamma_prev = c->gamma;
       c->beta = g / c->gamma;
+      c->zcoef = 1.0;
       c->iter += 1;
     }
     c->gamma = g;
@@ -300,7 +331,8 @@ __global__ void __launch_bounds__(BLOCK) k_self_blocks(BlockArgs a) {
 }
 
 // Gauss-Jordan inverse with partial pivoting per element; writes the
-// inverse structure-of-arrays binv[(i Np + j) ldb + k] in float64 and float32.
+// inverse, symmetrised and packed (upper triangle), structure-of-arrays
+// binv[sym_idx(i, j) ldb + k] in float64 and float32.
 template <int N, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_invert_blocks(BlockArgs a) {
   constexpr int Np = Dim<N>::Np;
@@ -342,10 +374,10 @@ __global__ void __launch_bounds__(BLOCK) k_invert_blocks(BlockArgs a) {
   }
   if (!ok) atomicOr(a.status, ST_BAD_INDEX);
   for (int i = 0; i < Np; ++i)
-    for (int j = 0; j < Np; ++j) {
-      const double v = ok ? m[i][Np + j] : NAN;
-      a.binv64[(size_t)(i * Np + j) * a.ldb + k] = v;
-      a.binv32[(size_t)(i * Np + j) * a.ldb + k] = (float)v;
+    for (int j = i; j < Np; ++j) {
+      const double v = ok ? 0.5 * (m[i][Np + j] + m[j][Np + i]) : NAN;
+      a.binv64[(size_t)sym_idx(Np, i, j) * a.ldb + k] = v;
+      a.binv32[(size_t)sym_idx(Np, i, j) * a.ldb + k] = (float)v;
     }
 }
 
@@ -368,7 +400,7 @@ __global__ void __launch_bounds__(BLOCK) k_pc_apply(const T* __restrict__ r, T* 
     for (int i = 0; i < Np; ++i) {
       T acc = T(0);
 #pragma unroll
-      for (int j = 0; j < Np; ++j) acc = fma(__ldg(binv + (size_t)(i * Np + j) * ldb + k), rv[j], acc);
+      for (int j = 0; j < Np; ++j) acc = fma(__ldg(binv + (size_t)sym_idx(Np, i, j) * ldb + k), rv[j], acc);
       s[tid * Np + i] = acc;
     }
   }
@@ -467,6 +499,35 @@ __global__ void __launch_bounds__(BLOCK) k_rhs(RhsArgs a) {
   for (int i = 0; i < Np; ++i) a.rhs[(size_t)k * Np + i] = y[i];
 }
 
+// ================================================= mixed precision helpers
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_cast_norm(int64_t n, const double* __restrict__ r64,
+                                                      float* __restrict__ r32, float* __restrict__ x32,
+                                                      double* part, CgCtl* ctl) {
+  __shared__ double s_red[64];
+  double s = 0.0, d = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * BLOCK) {
+    const float v = (float)r64[i];
+    r32[i] = v;
+    x32[i] = 0.0f;
+    s += (double)v * (double)v;
+  }
+  block_sum2<BLOCK>(s, d, s_red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (!is_last_block(&ctl->ticket)) return;
+  double t, u;
+  reduce_partials2<BLOCK>(part, nullptr, gridDim.x, t, u, s_red);
+  if (threadIdx.x == 0) {
+    ctl->bb = t;
+    ctl->ticket = 0u;
+  }
+}
+
+__global__ void k_axpy_mixed(int64_t n, const float* __restrict__ x32, double* __restrict__ x64) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x64[i] += (double)x32[i];
+}
+
 // ============================================================ vectors
 __global__ void k_axpby(int64_t n, double al, const double* __restrict__ x, double be, double* __restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -551,6 +612,7 @@ static cudaError_t launch_apply_n(int mode, const ApplyArgs<T>& a, cudaStream_t 
     case AM_APPLY: k_apply<N, T, AM_APPLY, B><<<grid, B, 0, s>>>(a); break;
     case AM_PFUSE: k_apply<N, T, AM_PFUSE, B><<<grid, B, 0, s>>>(a); break;
     case AM_RESID: k_apply<N, T, AM_RESID, B><<<grid, B, 0, s>>>(a); break;
+    case AM_SMOOTH: k_apply<N, T, AM_SMOOTH, B><<<grid, B, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -673,6 +735,15 @@ cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cuda
   return cudaGetLastError();
 }
 int dot_grid(int64_t n) { return vec_grid(n); }
+cudaError_t launch_cast_norm(int64_t n, const double* r64, float* r32, float* x32, double* part, CgCtl* ctl,
+                             cudaStream_t s) {
+  k_cast_norm<256><<<vec_grid(n), 256, 0, s>>>(n, r64, r32, x32, part, ctl);
+  return cudaGetLastError();
+}
+cudaError_t launch_axpy_mixed(int64_t n, const float* x32, double* x64, cudaStream_t s) {
+  k_axpy_mixed<<<vec_grid(n), 256, 0, s>>>(n, x32, x64);
+  return cudaGetLastError();
+}
 cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double* part, unsigned int* ticket,
                        double* out, cudaStream_t s) {
   const int g = vec_grid(n);

@@ -8,7 +8,7 @@ namespace ddg {
 
 struct CgCtl;
 
-enum ApplyMode { AM_APPLY = 0, AM_PFUSE = 1, AM_RESID = 2 };
+enum ApplyMode { AM_APPLY = 0, AM_PFUSE = 1, AM_RESID = 2, AM_SMOOTH = 3 };
 
 template <typename T>
 struct ApplyArgs {
@@ -28,6 +28,9 @@ struct ApplyArgs {
   double alpha;             // mass coefficient
   double shift;             // + shift * u
   int use_tma;              // all vector pointers 16-byte aligned
+  const T* binv;            // SMOOTH: packed block-Jacobi inverses (SoA)
+  int ldb;
+  double omega;             // SMOOTH: damping
 };
 
 template <typename T>
@@ -43,7 +46,9 @@ struct CgArgs {
   CgCtl* ctl;
   double* partA;
   double* partB;
+  double* partC;   // INIT with keep_p: r.p_old partials
   const unsigned int* dev_status;  // non-zero: a kernel reported an error
+  int keep_p;      // INIT: continue with the existing direction (reliable update)
   int K;
   int has_cond;
   cudaGraphConditionalHandle cond;
@@ -82,8 +87,27 @@ cudaError_t launch_pc_apply(int N, const T* r, T* z, const T* binv, int ldb, int
 cudaError_t launch_rhs(int N, const RhsArgs& a, cudaStream_t s);
 cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, double* y, cudaStream_t s);
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s);
+// r32 = float(r64), x32 = 0, ctl->bb = r32.r32 (reliable-update restart)
+cudaError_t launch_cast_norm(int64_t n, const double* r64, float* r32, float* x32, double* part, CgCtl* ctl,
+                             cudaStream_t s);
+// x64 += double(x32)
+cudaError_t launch_axpy_mixed(int64_t n, const float* x32, double* x64, cudaStream_t s);
 cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double* part, unsigned int* ticket,
                        double* out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_elem_matvec(int Kout, int rows, int cols, const T* M, const T* in, T* out, int add,
+                               cudaStream_t s);
+template <typename T>
+cudaError_t launch_dense_gemv(int n, const T* A, const T* b, T* x, cudaStream_t s);
+template <typename T>
+cudaError_t launch_bj_scaled(int N, const T* b, T* x, const T* binv, int ldb, int K, T scale, cudaStream_t s);
+template <typename T>
+cudaError_t launch_cg_xr(T* x, const T* p, T* r, const T* Ap, int64_t n, CgCtl* ctl, double* part, cudaStream_t s);
+template <typename T>
+cudaError_t launch_cg_finish(bool init, const T* r, const T* z, int64_t n, CgCtl* ctl, double* part,
+                             const unsigned int* dev_status, int has_cond, cudaGraphConditionalHandle cond,
+                             cudaStream_t s);
+int xr_grid(int64_t n);
 int apply_grid(int K);
 int cg_grid(int K);
 int dot_grid(int64_t n);

@@ -156,6 +156,32 @@ class SipgOperator:
         return _lib.SOLVE_STATUS.get(info.status, str(info.status)), info.iterations, info.res_norm2, info.b_norm2
 
 
+    def cg_mixed(self, b, x, *, tol=1e-9, atol=0.0, maxiter=1000, pc=False, alpha=0.0, shift=0.0,
+                 delta=0.1, stream=None):
+        """Mixed-precision CG with float64 reliable updates (float64 b, x;
+        x holds x0 and is overwritten).  Returns (status, float32 iterations,
+        float64 r.r, b.b, reliable updates)."""
+        info = _lib.SolveInfo()
+        cfg = _lib.CgConfig(tol=float(tol), atol=float(atol), maxiter=int(maxiter),
+                            pc=_lib.DDG_PC_JACOBI if pc else _lib.DDG_PC_NONE,
+                            alpha=float(alpha), shift=float(shift), precision=_lib.DDG_FP32, reserved=0)
+        _lib.check(_lib.lib().ddg_sipg_cg_mixed(self._h, C.byref(cfg), float(delta), b.data_ptr(), x.data_ptr(),
+                                                _lib.stream_handle(stream), C.byref(info)), "ddg_sipg_cg_mixed")
+        return (_lib.SOLVE_STATUS.get(info.status, str(info.status)), info.iterations, info.res_norm2,
+                info.b_norm2, info.updates)
+
+
+    def cg_mg(self, mg, b, x, *, tol=1e-9, atol=0.0, maxiter=1000, alpha=0.0, shift=0.0, stream=None):
+        """float64 CG preconditioned by the device V-cycle ``mg`` (float64 b,
+        x; x holds x0, overwritten).  Returns (status, iterations, r.r, b.b)."""
+        info = _lib.SolveInfo()
+        cfg = _lib.CgConfig(tol=float(tol), atol=float(atol), maxiter=int(maxiter), pc=0,
+                            alpha=float(alpha), shift=float(shift), precision=_lib.DDG_FP64, reserved=0)
+        _lib.check(_lib.lib().ddg_sipg_cg_mg(self._h, C.byref(cfg), mg._h, b.data_ptr(), x.data_ptr(),
+                                             _lib.stream_handle(stream), C.byref(info)), "ddg_sipg_cg_mg")
+        return _lib.SOLVE_STATUS.get(info.status, str(info.status)), info.iterations, info.res_norm2, info.b_norm2
+
+
 def dot(x, y, stream=None) -> float:
     """x . y with float64 accumulation (device kernel), returned to the host."""
     import torch

@@ -9,9 +9,13 @@ shape ``(Np, K)``.
 
 Differences (extensions, all opt-in):
   * ``IterativeConfig`` accepts ``method="gmres"`` (restarted GMRES,
-    ``restart``) and ``precision="mixed"`` (float32 inner CG inside a float64
-    iterative-refinement loop, ``inner_tol``); the defaults reproduce the
-    reference (``method="cg"``, float64).
+    ``restart``) and ``precision="mixed"``: float32 PCG iterations that keep
+    their search direction across float64 residual replacements (reliable
+    updates, every ``inner_tol`` reduction of the float32 residual), so the
+    iteration count stays near the float64 one and the result is float64
+    accurate.  ``precision="mixed-restart"`` is plain iterative refinement
+    (float32 CG restarted from each float64 residual).  The defaults
+    reproduce the reference (``method="cg"``, float64).
   * Solves can return their Krylov status (``return_info=True``): the
     reference discards jax's ``info`` (``sipg.py:604,910``).
   * ``cub`` (curved-element cubature) is not supported: a ValueError.
@@ -39,9 +43,9 @@ class IterativeConfig:
     tol: float = 1e-9
     atol: float = 0.0
     maxiter: int = 1000
-    precision: str = "fp64"      # "fp64" | "mixed"
-    inner_tol: float = 1e-4      # mixed: relative tolerance of each float32 inner solve
-    max_refinements: int = 50    # mixed: outer iteration cap
+    precision: str = "fp64"      # "fp64" | "mixed" | "mixed-restart"
+    inner_tol: float = 0.1       # mixed: float32 residual reduction between float64 updates
+    max_refinements: int = 50    # mixed-restart: outer iteration cap
     restart: int = 30            # gmres
 
 
@@ -335,7 +339,7 @@ def _mixed_ir(op, b, x, *, alpha, shift, cfg, pc):
             break
         r32 = cast(r, torch.float32)
         d32 = torch.zeros_like(r32)
-        st, its, _, _ = op.cg(r32, d32, tol=cfg.inner_tol, atol=0.0, maxiter=cfg.maxiter - total_inner,
+        st, its, _, _ = op.cg(r32, d32, tol=1e-4, atol=0.0, maxiter=cfg.maxiter - total_inner,
                               pc=pc, alpha=alpha, shift=shift, precision="fp32")
         total_inner += its
         if st == "breakdown" or its == 0:
@@ -353,10 +357,16 @@ def _iterative_solve(mesh, op, b, x0, *, alpha, shift, iterative, preconditioner
     x = torch.zeros_like(b) if x0 is None else _flat(x0, b.device)
     if iterative.method not in ("cg", "gmres"):
         raise ValueError(f"iterative method {iterative.method!r} not supported for SPD")
-    if iterative.precision not in ("fp64", "mixed"):
-        raise ValueError(f"precision {iterative.precision!r} must be 'fp64' or 'mixed'")
+    if iterative.precision not in ("fp64", "mixed", "mixed-restart"):
+        raise ValueError(f"precision {iterative.precision!r} must be 'fp64', 'mixed' or 'mixed-restart'")
+    from .multigrid import SipgMultigrid
     native_pc = preconditioner is None or (
         isinstance(preconditioner, BlockJacobiPreconditioner) and preconditioner.valid_for(op, alpha))
+    if isinstance(preconditioner, SipgMultigrid) and preconditioner.matches(op, alpha) \
+            and iterative.method == "cg" and iterative.precision == "fp64":
+        st, its, rr, bb = op.cg_mg(preconditioner, b, x, tol=iterative.tol, atol=iterative.atol,
+                                   maxiter=iterative.maxiter, alpha=alpha, shift=shift)
+        return x, SolveInfo(st, its, float(np.sqrt(max(rr, 0.0))), float(np.sqrt(bb)))
     use_pc = preconditioner is not None
     if iterative.method == "gmres":
         from .krylov import gmres
@@ -364,11 +374,17 @@ def _iterative_solve(mesh, op, b, x0, *, alpha, shift, iterative, preconditioner
         info = gmres(op, b, x, alpha=alpha, shift=shift, tol=iterative.tol, atol=iterative.atol,
                      maxiter=iterative.maxiter, restart=iterative.restart, M=M)
         return x, info
-    if iterative.precision == "mixed":
+    if iterative.precision in ("mixed", "mixed-restart"):
         if not native_pc:
-            raise ValueError("precision='mixed' needs no preconditioner or a block-Jacobi one built on "
+            raise ValueError("mixed precision needs no preconditioner or a block-Jacobi one built on "
                              "the same mesh, BC tags, penalty and alpha")
-        return x, _mixed_ir(op, b, x, alpha=alpha, shift=shift, cfg=iterative, pc=use_pc)
+        if iterative.precision == "mixed-restart":
+            return x, _mixed_ir(op, b, x, alpha=alpha, shift=shift, cfg=iterative, pc=use_pc)
+        st, its, rr, bb, upd = op.cg_mixed(b, x, tol=iterative.tol, atol=iterative.atol,
+                                           maxiter=iterative.maxiter, pc=use_pc, alpha=alpha, shift=shift,
+                                           delta=iterative.inner_tol)
+        return x, SolveInfo(st, its, float(np.sqrt(max(rr, 0.0))), float(np.sqrt(bb)), refinements=upd,
+                            inner_iterations=its)
     if native_pc:
         st, its, rr, bb = op.cg(b, x, tol=iterative.tol, atol=iterative.atol, maxiter=iterative.maxiter,
                                 pc=use_pc, alpha=alpha, shift=shift, precision="fp64")

@@ -139,9 +139,11 @@ typedef struct {
 
 typedef struct {
     int32_t status;      /* DDG_SOLVE_*                                     */
-    int32_t iterations;
-    double  res_norm2;   /* final r.r (preconditioned: r.r; else r.z = r.r) */
+    int32_t iterations;  /* CG iterations (mixed: float32 iterations)       */
+    double  res_norm2;   /* final r.r (mixed: float64 true residual)        */
     double  b_norm2;     /* b.b                                             */
+    int32_t updates;     /* mixed: float64 reliable updates performed       */
+    int32_t reserved;
 } ddg_solve_info;
 
 /* CG on (alpha M + A + shift I) x = b with the stopping rule of
@@ -153,6 +155,58 @@ typedef struct {
  * after the stream has been synchronised and `info` filled. */
 int ddg_sipg_cg(ddg_sipg_op *op, const ddg_cg_config *cfg, const void *b,
                 void *x, void *stream, ddg_solve_info *info);
+
+/* Mixed-precision CG with reliable updates (extension; the reference solves
+ * in float64 only).  float32 PCG iterations (operator, vectors and
+ * block-Jacobi in float32, dot products accumulated in float64) keep their
+ * search direction across float64 residual replacements: whenever the
+ * float32 residual has dropped by `delta` (e.g. 0.1) since the last
+ * replacement, x += x32, r = b - A x is recomputed in float64 and the
+ * float32 iteration continues from it.  Stops when the float64 residual
+ * satisfies the cfg tolerances (same rule as ddg_sipg_cg), after
+ * cfg->maxiter float32 iterations, or when replacements stop reducing the
+ * float64 residual (status DDG_SOLVE_STAGNATED).  cfg->precision is ignored.
+ * b, x: float64 device vectors (x: x0 in, solution out). */
+#define DDG_SOLVE_STAGNATED  4
+int ddg_sipg_cg_mixed(ddg_sipg_op *op, const ddg_cg_config *cfg, double delta,
+                      const double *b, double *x, void *stream, ddg_solve_info *info);
+
+/* ---- p / hp multigrid (src/ddg/dg2d/multigrid.py) ---------------------- */
+typedef struct ddg_mg ddg_mg;                /* opaque, library-owned */
+
+/* V-cycle description.  Level l = 0 is the finest.  Every level handle must
+ * have its block-Jacobi smoother built with ddg_sipg_pc_build(alpha).
+ * Between levels l and l+1 the transfer is either a p-transfer (same K,
+ * prolongation I of shape (Np_l, Np_{l+1}), multigrid.py:106-134) or an
+ * h-transfer (K_l = 4 K_{l+1}, fine element 4k+c = child c of k,
+ * prolongation [I_0; I_1; I_2; I_3] of shape (4 Np, Np), :137-184).
+ * Restriction is the transpose.  coarse_inv is the dense inverse of the
+ * coarsest operator (the reference LU-factors it, :220-228; the caller
+ * adds its eps*max|diag| shift first when regularising).  All HOST arrays,
+ * read during the call. */
+typedef struct {
+    int32_t nlevels;
+    int32_t precision;        /* DDG_FP32 or DDG_FP64: smoothing, transfers, coarse */
+    int32_t nu;               /* pre/post smoothing sweeps (nu_smooth)      */
+    int32_t reserved;
+    double  omega;            /* smoother damping                            */
+    double  alpha;            /* level operators are alpha M + A             */
+    ddg_sipg_op *const *ops;  /* nlevels handles, finest first               */
+    const double *const *prolong;   /* nlevels-1 host row-major matrices     */
+    const int32_t *prolong_rows, *prolong_cols;
+    const double *coarse_inv; /* (nc, nc) row-major, nc = K*Np of the coarsest */
+} ddg_mg_desc;
+
+int ddg_mg_create(const ddg_mg_desc *desc, ddg_mg **out);
+int ddg_mg_destroy(ddg_mg *mg);
+/* z = V-cycle(r) (multigrid.py:232-246), float64 device vectors of the
+ * finest level (the M^-1(v_flat) callable of make_sipg_(hp)mg_preconditioner). */
+int ddg_mg_apply(ddg_mg *mg, const double *r, double *z, void *stream);
+/* float64 CG on (alpha M + A + shift I) x = b preconditioned by one V-cycle
+ * per iteration; the whole loop, V-cycle included, runs as one device graph.
+ * Stopping rule as ddg_sipg_cg (preconditioned: on r.r). */
+int ddg_sipg_cg_mg(ddg_sipg_op *op, const ddg_cg_config *cfg, ddg_mg *mg,
+                   const double *b, double *x, void *stream, ddg_solve_info *info);
 
 /* ---- small vector helpers (device) ------------------------------------ */
 /* y = a*x + b*y  (float64) */
