@@ -213,6 +213,18 @@ int ddg_sipg_cg_mg(ddg_sipg_op *op, const ddg_cg_config *cfg, ddg_mg *mg,
 int ddg_axpby(int64_t n, double a, const double *x, double b, double *y, void *stream);
 /* out[0] = x.y  (float64 accumulation), out device double */
 int ddg_dot(int64_t n, int precision, const void *x, const void *y, double *out, void *stream);
+/* out[0] = x.y without allocating: no counterpart in the reference (an
+ * addition for callers that cannot allocate device memory, e.g. code being
+ * captured into a CUDA graph, or an embedding application that owns a fixed
+ * device-memory budget).  Its scratch (block partials and a completion
+ * counter, 512 KiB) is a static device array inside this library, present
+ * on every GPU that has called it until the process exits.  n must not
+ * exceed DDG_DOT_NOALLOC_MAX_N.  The first call on a device looks up that
+ * array's address (do it before any stream capture); every call clears the
+ * counter on `stream` first; calls that overlap on the GPU share the array
+ * and race.  Same float64 accumulation as ddg_dot (summation order differs). */
+#define DDG_DOT_NOALLOC_MAX_N 536870912LL
+int ddg_dot_noalloc(int64_t n, int precision, const void *x, const void *y, double *out, void *stream);
 /* float64 <-> float32 copies */
 int ddg_cast(int64_t n, int to_precision, const void *src, void *dst, void *stream);
 
