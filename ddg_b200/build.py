@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libddg_sipg.so")
 
-CU_SOURCES = ["sipg_kernels.cu", "sipg_mg.cu", "sipg_capi.cu", "noalloc.cu"]
+CU_SOURCES = ["sipg_kernels.cu", "sipg_mg.cu", "sipg_capi.cu", "sipg_pool.cu", "noalloc.cu"]
 CXX_SOURCES = ["mesh_connect.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

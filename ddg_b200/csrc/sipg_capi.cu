@@ -107,12 +107,17 @@ struct ddg_sipg_op {
 
 namespace {
 
-int build_nbr(ddg_sipg_op* op, const int32_t* bc) {
-  const int K = op->K, N = op->N, Np = op->Np, Nfp = op->Nfp;
-  op->nbr_host.assign((size_t)3 * K, 0u);
+}  // namespace
+
+// Neighbour words of K elements (nbr_pack layout, out[f * out_ld + k]);
+// element ids inside the words are shifted by k_offset (pools place a
+// request's elements at [k_offset, k_offset + K)).
+int ddg::pack_neighbours(int K, int N, const int64_t* EToE, const int64_t* EToF, const int64_t* vmapP,
+                         const int64_t* rot, const int32_t* bc, uint32_t k_offset, uint32_t* out, size_t out_ld) {
+  const int Np = (N + 1) * (N + 2) / 2, Nfp = N + 1;
   for (int k = 0; k < K; ++k)
     for (int f = 0; f < 3; ++f) {
-      const int64_t kp = op->EToE[(size_t)k * 3 + f], fp = op->EToF[(size_t)k * 3 + f];
+      const int64_t kp = EToE[(size_t)k * 3 + f], fp = EToF[(size_t)k * 3 + f];
       const int tag = bc[(size_t)k * 3 + f];
       if (tag < 0 || tag > 2) return fail(DDG_ERR_INVALID, "bc_types entries must be 0, 1 or 2");
       if (kp < 0 || kp >= K || fp < 0 || fp > 2) return fail(DDG_ERR_INVALID, "EToE/EToF out of range");
@@ -125,12 +130,12 @@ int build_nbr(ddg_sipg_op* op, const int32_t* bc) {
         // node order of the partner face (re-labelled so its face is face 0)
         int nsame = 0, nrev = 0;
         for (int p = 0; p < Nfp; ++p) {
-          const int64_t j = op->vmapP[((size_t)k * 3 + f) * Nfp + p];
+          const int64_t j = vmapP[((size_t)k * 3 + f) * Nfp + p];
           if (j / Np != kp) return fail(DDG_ERR_INVALID, "vmapP does not point into the EToE neighbour (non-conforming face)");
           const int64_t loc = j % Np;
           int q = -1;
           for (int qq = 0; qq < Nfp; ++qq)
-            if (op->rot[(size_t)fp * Np + qq] == loc) q = qq;
+            if (rot[(size_t)fp * Np + qq] == loc) q = qq;
           if (q == p) ++nsame;
           if (q == N - p) ++nrev;
         }
@@ -139,9 +144,18 @@ int build_nbr(ddg_sipg_op* op, const int32_t* bc) {
       }
       // a self-pointing face tagged interior contributes nothing (its jump
       // vanishes and its two scatters cancel: sipg.py:241-249)
-      op->nbr_host[(size_t)f * K + k] = nbr_pack((uint32_t)kp, (uint32_t)fp, flip, (uint32_t)tag, pact, mint);
+      out[(size_t)f * out_ld + k] =
+          nbr_pack((uint32_t)(kp + k_offset), (uint32_t)fp, flip, (uint32_t)tag, pact, mint);
     }
   return DDG_OK;
+}
+
+namespace {
+
+int build_nbr(ddg_sipg_op* op, const int32_t* bc) {
+  op->nbr_host.assign((size_t)3 * op->K, 0u);
+  return ddg::pack_neighbours(op->K, op->N, op->EToE.data(), op->EToF.data(), op->vmapP.data(), op->rot.data(), bc, 0u,
+                         op->nbr_host.data(), (size_t)op->K);
 }
 
 int ensure_work(ddg_sipg_op* op, int prec) {
@@ -292,6 +306,37 @@ void free_op(ddg_sipg_op* op) {
 extern "C" const char* ddg_last_error(void) { return g_err.c_str(); }
 extern "C" const char* ddg_version(void) { return "ddg_sipg 0.1 (sm_100a)"; }
 
+// Reference-element matrices of degree N into constant memory of `device`
+// (once per device and degree; later calls must pass the same matrices).
+extern "C" int ddg_sipg_upload_reference(int N, const double* Dr, const double* Ds, const double* M,
+                                         const double* m1d, int device) {
+  if (N < 1 || N > DDG_MAX_DEGREE || !Dr || !Ds || !M || !m1d)
+    return fail(DDG_ERR_INVALID, "reference matrices: bad arguments");
+  const int Np = (N + 1) * (N + 2) / 2, Nfp = N + 1;
+  std::lock_guard<std::mutex> lk(g_ref_mu);
+  std::vector<double> blob;
+  blob.insert(blob.end(), Dr, Dr + Np * Np);
+  blob.insert(blob.end(), Ds, Ds + Np * Np);
+  blob.insert(blob.end(), M, M + Np * Np);
+  blob.insert(blob.end(), m1d, m1d + 3 * Nfp * Nfp);
+  auto key = std::make_pair(device, N);
+  auto it = g_ref_loaded.find(key);
+  if (it == g_ref_loaded.end()) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    cudaError_t e = upload_ref(N, Dr, Ds, M, m1d);
+    cudaSetDevice(cur);
+    if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("constant upload: ") + cudaGetErrorString(e));
+    g_ref_loaded[key] = blob;
+    return DDG_OK;
+  }
+  for (size_t i = 0; i < blob.size(); ++i)
+    if (std::fabs(blob[i] - it->second[i]) > 1e-12 * (1.0 + std::fabs(blob[i])))
+      return fail(DDG_ERR_INVALID, "reference matrices differ from the ones already loaded for this degree");
+  return DDG_OK;
+}
+
 extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
   if (!d || !out) return fail(DDG_ERR_INVALID, "ddg_sipg_create: null argument");
   *out = nullptr;
@@ -348,27 +393,10 @@ extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
   }
   // constant memory (once per device and degree)
   {
-    std::lock_guard<std::mutex> lk(g_ref_mu);
-    std::vector<double> blob;
-    blob.insert(blob.end(), d->Dr, d->Dr + Np * Np);
-    blob.insert(blob.end(), d->Ds, d->Ds + Np * Np);
-    blob.insert(blob.end(), d->M, d->M + Np * Np);
-    blob.insert(blob.end(), d->m1d, d->m1d + 3 * Nfp * Nfp);
-    auto key = std::make_pair(d->device, N);
-    auto it = g_ref_loaded.find(key);
-    if (it == g_ref_loaded.end()) {
-      cudaError_t e = upload_ref(N, d->Dr, d->Ds, d->M, d->m1d);
-      if (e != cudaSuccess) {
-        free_op(op);
-        return fail(DDG_ERR_CUDA, std::string("constant upload: ") + cudaGetErrorString(e));
-      }
-      g_ref_loaded[key] = blob;
-    } else {
-      for (size_t i = 0; i < blob.size(); ++i)
-        if (std::fabs(blob[i] - it->second[i]) > 1e-12 * (1.0 + std::fabs(blob[i]))) {
-          free_op(op);
-          return fail(DDG_ERR_INVALID, "reference matrices differ from the ones already loaded for this degree");
-        }
+    const int urc = ddg_sipg_upload_reference(N, d->Dr, d->Ds, d->M, d->m1d, d->device);
+    if (urc != DDG_OK) {
+      free_op(op);
+      return urc;
     }
   }
   // geometry (SoA, float64 and float32)

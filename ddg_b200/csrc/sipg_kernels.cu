@@ -313,20 +313,23 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
 template <int N, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_self_blocks(BlockArgs a) {
   constexpr int Np = Dim<N>::Np;
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
-  if (k >= a.K) return;
+  const int kl = blockIdx.x * BLOCK + threadIdx.x;
+  if (kl >= a.K) return;
+  const int k = a.k0 + kl;
+  const size_t ld = a.nbr_ld ? (size_t)a.nbr_ld : (size_t)a.K;
   uint32_t w[3];
 #pragma unroll
-  for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
+  for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * ld + k);
   const Geo<double> g = load_geo(a.geo, a.ldg, k);
+  const double al = a.alpha_e ? a.alpha_e[k] : a.alpha;
   NbrZero<double, Np> src;
   for (int j = 0; j < Np; ++j) {
     double u[Np], y[Np];
 #pragma unroll
     for (int i = 0; i < Np; ++i) u[i] = (i == j) ? 1.0 : 0.0;
-    elem_apply<N, double, false>(u, y, g, w, a.geo, a.ldg, a.tau, a.alpha, src);
+    elem_apply<N, double, false>(u, y, g, w, a.geo, a.ldg, a.tau, al, src);
 #pragma unroll
-    for (int i = 0; i < Np; ++i) a.blocks[(size_t)k * Np * Np + i * Np + j] = y[i] + (i == j ? a.shift : 0.0);
+    for (int i = 0; i < Np; ++i) a.blocks[(size_t)kl * Np * Np + i * Np + j] = y[i] + (i == j ? a.shift : 0.0);
   }
 }
 
@@ -336,12 +339,13 @@ __global__ void __launch_bounds__(BLOCK) k_self_blocks(BlockArgs a) {
 template <int N, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_invert_blocks(BlockArgs a) {
   constexpr int Np = Dim<N>::Np;
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
-  if (k >= a.K) return;
+  const int kl = blockIdx.x * BLOCK + threadIdx.x;
+  if (kl >= a.K) return;
+  const int k = a.k0 + kl;
   double m[Np][2 * Np];
   for (int i = 0; i < Np; ++i)
     for (int j = 0; j < Np; ++j) {
-      m[i][j] = a.blocks[(size_t)k * Np * Np + i * Np + j];
+      m[i][j] = a.blocks[(size_t)kl * Np * Np + i * Np + j];
       m[i][Np + j] = (i == j) ? 1.0 : 0.0;
     }
   bool ok = true;
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(BLOCK) k_invert_blocks(BlockArgs a) {
     for (int j = i; j < Np; ++j) {
       const double v = ok ? 0.5 * (m[i][Np + j] + m[j][Np + i]) : NAN;
       a.binv64[(size_t)sym_idx(Np, i, j) * a.ldb + k] = v;
-      a.binv32[(size_t)sym_idx(Np, i, j) * a.ldb + k] = (float)v;
+      if (a.binv32) a.binv32[(size_t)sym_idx(Np, i, j) * a.ldb + k] = (float)v;
     }
 }
 
@@ -753,3 +757,5 @@ cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double
 }
 
 }  // namespace ddg
+
+#include "sipg_batch_kernels.cuh"

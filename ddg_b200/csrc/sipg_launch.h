@@ -57,12 +57,36 @@ struct CgArgs {
 struct BlockArgs {
   const double* geo;
   const uint32_t* nbr;
-  double* blocks;     // (K, Np, Np)
-  double* binv64;     // SoA
-  float* binv32;
+  double* blocks;     // (K, Np, Np) for elements k0 .. k0+K-1
+  double* binv64;     // SoA, indexed by the global element id
+  float* binv32;      // (may be null)
   unsigned int* status;
   int K, ldg, ldb;
   double tau, alpha, shift;
+  int k0;             // first element
+  int nbr_ld;         // element stride of the neighbour words (0: K)
+  const double* alpha_e;  // per-element alpha (overrides alpha when set)
+};
+
+// Continuous-batching pool: per-request CG state on the device.
+struct BatchReq {
+  int k0, K, active, iter, maxiter, status, pad0, pad1;
+  double gamma, gamma_prev, pAp, alpha, beta, rr, bb, tol2, atol_sq, atol2;
+};
+
+struct BatchArgs {
+  int cap, hw;             // element capacity (SoA stride) and launch range
+  const double* geo;       // SoA [14][cap]
+  const uint32_t* nbr;     // [3][cap]
+  const int* seg;          // [cap] request slot of each element, -1 when free
+  const double* alpha_e;   // [cap] Helmholtz coefficient of each element
+  const double* binv;      // packed block-Jacobi inverses, SoA [Np(Np+1)/2][cap]
+  double *x, *b, *r, *z, *Ap;
+  double *epA, *epB;       // per-element partial sums
+  BatchReq* req;
+  const int* perm;
+  double tau;
+  int max_req;
 };
 
 struct RhsArgs {
@@ -108,6 +132,14 @@ cudaError_t launch_cg_finish(bool init, const T* r, const T* z, int64_t n, CgCtl
                              const unsigned int* dev_status, int has_cond, cudaGraphConditionalHandle cond,
                              cudaStream_t s);
 int xr_grid(int64_t n);
+cudaError_t launch_batch_pfuse(int N, const BatchArgs& a, const double* pin, double* pout, cudaStream_t s);
+cudaError_t launch_batch_step(int N, const BatchArgs& a, const double* p, cudaStream_t s);
+cudaError_t launch_batch_seg(int mode, const BatchArgs& a, int first_req, int nreq, cudaStream_t s);
+cudaError_t launch_batch_init(int N, const BatchArgs& a, double* p0, int k0, int K, cudaStream_t s);
+cudaError_t launch_batch_rhs(int N, const BatchArgs& a, const double* f, int k0, int K, cudaStream_t s);
+// host: neighbour words of a mesh, element ids shifted by k_offset
+int pack_neighbours(int K, int N, const int64_t* EToE, const int64_t* EToF, const int64_t* vmapP,
+                    const int64_t* rot, const int32_t* bc, uint32_t k_offset, uint32_t* out, size_t out_ld);
 int apply_grid(int K);
 int cg_grid(int K);
 int dot_grid(int64_t n);

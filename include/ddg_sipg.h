@@ -208,6 +208,38 @@ int ddg_mg_apply(ddg_mg *mg, const double *r, double *z, void *stream);
 int ddg_sipg_cg_mg(ddg_sipg_op *op, const ddg_cg_config *cfg, ddg_mg *mg,
                    const double *b, double *x, void *stream, ddg_solve_info *info);
 
+/* ---- continuous-batching solve pool (serving) ------------------------- */
+/* Extension (the reference solves one mesh per call).  A pool packs many
+ * independent solves of one degree N into one element array; every CG
+ * scalar is per request (segmented reductions), so a request's iterates are
+ * the same whichever other requests share the launches.  The caller runs
+ * the scheduling loop: admit arrivals while others iterate, iterate, poll,
+ * retire finished requests (their element range is reused at once). */
+typedef struct ddg_pool ddg_pool;
+
+/* capacity: element slots (device memory is sized from it);
+ * max_requests: concurrent requests; max_request_K: largest request. */
+int ddg_pool_create(int N, int capacity, int max_requests, int max_request_K,
+                    double tau_scale, int device, ddg_pool **out);
+int ddg_pool_destroy(ddg_pool *pool);
+/* Admit one (alpha M + A) u = J M f solve on `mesh` (host arrays, its own
+ * numbering; bc_types as in ddg_sipg_mesh_desc), source f (K x Np,
+ * element-major, host), CG tolerances.  Returns the request slot, or
+ * DDG_ERR_NOMEM when no slot / element range is free right now. */
+int ddg_pool_admit(ddg_pool *pool, const ddg_sipg_mesh_desc *mesh, double alpha,
+                   double tol, double atol, int maxiter, const double *f,
+                   void *stream, int *slot);
+/* 2*pairs block-Jacobi PCG iterations of every active request (one graph). */
+int ddg_pool_iterate(ddg_pool *pool, int pairs, void *stream);
+/* Per slot: 1 while iterating, 0 when finished or empty; iteration counts. */
+int ddg_pool_poll(ddg_pool *pool, int32_t *active, int32_t *iterations, void *stream);
+/* Copy a finished request's solution (K x Np, host) and free its slot. */
+int ddg_pool_retire(ddg_pool *pool, int slot, double *x, void *stream, ddg_solve_info *info);
+/* Reference-element matrices of degree N into `device`'s constant memory
+ * (ddg_sipg_create does this itself). */
+int ddg_sipg_upload_reference(int N, const double *Dr, const double *Ds, const double *M,
+                              const double *m1d, int device);
+
 /* ---- small vector helpers (device) ------------------------------------ */
 /* y = a*x + b*y  (float64) */
 int ddg_axpby(int64_t n, double a, const double *x, double b, double *y, void *stream);
