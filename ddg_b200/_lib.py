@@ -86,6 +86,8 @@ _PROTOS = {
     "ddg_pool_poll": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ddg_pool_retire": (C.c_int, [_vp, C.c_int, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_sipg_upload_reference": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, C.c_int]),
+    "ddg_sipg_set_kappa": (C.c_int, [_vp, _vp]),
+    "ddg_sipg_grad_kappa": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "ddg_axpby": (C.c_int, [_i64, C.c_double, _vp, C.c_double, _vp, _vp]),
     "ddg_dot": (C.c_int, [_i64, C.c_int, _vp, _vp, _vp, _vp]),
     "ddg_cast": (C.c_int, [_i64, C.c_int, _vp, _vp, _vp]),

@@ -90,6 +90,9 @@ struct ddg_sipg_op {
   unsigned int* ticket = nullptr;   // for the free dot helper
   double* dotbuf = nullptr;
   // block Jacobi
+  double* kappa64 = nullptr;        // per-element diffusivity (extension)
+  float* kappa32 = nullptr;
+  bool kappa_on = false;
   double* blocks = nullptr;
   double* binv64 = nullptr;
   float* binv32 = nullptr;
@@ -189,6 +192,7 @@ ApplyArgs<T> apply_args(ddg_sipg_op* op) {
   a.K = op->K;
   a.ldg = op->ldg;
   a.tau = op->tau;
+  a.kappa = op->kappa_on ? ((sizeof(T) == 8) ? (const T*)op->kappa64 : (const T*)op->kappa32) : nullptr;
   return a;
 }
 
@@ -287,7 +291,7 @@ void free_op(ddg_sipg_op* op) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
   }
-  void* ptrs[] = {op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
+  void* ptrs[] = {op->kappa64, op->kappa32, op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
                   op->ticket, op->dotbuf, op->blocks, op->binv64, op->binv32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -490,6 +494,8 @@ extern "C" int ddg_sipg_apply(ddg_sipg_op* op, int prec, double alpha, const voi
 extern "C" int ddg_sipg_rhs(ddg_sipg_op* op, const double* f, const double* u_dir, const double* q_neu,
                             double* rhs, void* stream) {
   if (!op || !rhs) return fail(DDG_ERR_INVALID, "ddg_sipg_rhs: null argument");
+  if (op->kappa_on && u_dir)
+    return fail(DDG_ERR_UNSUPPORTED, "ddg_sipg_rhs: non-homogeneous Dirichlet data with a diffusivity is not built");
   DevGuard guard(op->dev);
   RhsArgs a{};
   a.geo = op->geo64;
@@ -529,6 +535,7 @@ extern "C" int ddg_sipg_pc_build(ddg_sipg_op* op, double alpha, void* stream) {
   a.tau = op->tau;
   a.alpha = alpha;
   a.shift = 0.0;
+  a.kappa = op->kappa_on ? op->kappa64 : nullptr;
   cudaError_t e = launch_block_jacobi(op->N, a, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("block-Jacobi launch: ") + cudaGetErrorString(e));
   CK(cudaStreamSynchronize((cudaStream_t)stream));
@@ -1185,5 +1192,65 @@ extern "C" int ddg_sipg_cg_mg(ddg_sipg_op* op, const ddg_cg_config* cfg, ddg_mg*
     info->b_norm2 = res.bb;
     info->updates = 0;
   }
+  return DDG_OK;
+}
+
+namespace {
+void drop_graphs(ddg_sipg_op* op) {
+  for (auto& kv : op->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.g) cudaGraphDestroy(kv.second.g);
+  }
+  op->graphs.clear();
+  for (auto& kv : op->mg_graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.g) cudaGraphDestroy(kv.second.g);
+  }
+  op->mg_graphs.clear();
+}
+}  // namespace
+
+extern "C" int ddg_sipg_set_kappa(ddg_sipg_op* op, const double* kappa) {
+  if (!op) return fail(DDG_ERR_INVALID, "ddg_sipg_set_kappa: null handle");
+  DevGuard guard(op->dev);
+  const bool on = kappa != nullptr;
+  if (on) {
+    for (int k = 0; k < op->K; ++k)
+      if (!(kappa[k] > 0.0) || !std::isfinite(kappa[k]))
+        return fail(DDG_ERR_INVALID, "ddg_sipg_set_kappa: diffusivity must be positive and finite");
+    if (!op->kappa64) {
+      CK(cudaMalloc((void**)&op->kappa64, (size_t)op->K * 8));
+      CK(cudaMalloc((void**)&op->kappa32, (size_t)op->K * 4));
+    }
+    std::vector<float> k32(kappa, kappa + op->K);
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(op->kappa64, kappa, (size_t)op->K * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(op->kappa32, k32.data(), (size_t)op->K * 4, cudaMemcpyHostToDevice));
+  }
+  if (on != op->kappa_on) {
+    CK(cudaDeviceSynchronize());
+    drop_graphs(op);          // captured launches bake the diffusivity pointer in
+  }
+  op->kappa_on = on;
+  op->pc_ready = false;       // the diagonal blocks depend on the diffusivity
+  return DDG_OK;
+}
+
+extern "C" int ddg_sipg_grad_kappa(ddg_sipg_op* op, const double* u, const double* lam, double* g, void* stream) {
+  if (!op || !u || !lam || !g) return fail(DDG_ERR_INVALID, "ddg_sipg_grad_kappa: null argument");
+  DevGuard guard(op->dev);
+  GradArgs a{};
+  a.geo = op->geo64;
+  a.nbr = op->nbr;
+  a.perm = op->perm;
+  a.u = u;
+  a.lam = lam;
+  a.kappa = op->kappa_on ? op->kappa64 : nullptr;
+  a.g = g;
+  a.K = op->K;
+  a.ldg = op->ldg;
+  a.tau = op->tau;
+  cudaError_t e = launch_grad_kappa(op->N, a, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("ddg_sipg_grad_kappa: ") + cudaGetErrorString(e));
   return DDG_OK;
 }

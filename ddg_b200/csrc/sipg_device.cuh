@@ -264,12 +264,19 @@ struct NbrZero {  // self-block extraction: the neighbour carries no value
 // y = A u + alpha J M u  for element k (u, y in registers).
 // USE_NBR=false skips the neighbour value gather (self-block mode: the
 // neighbour's value is zero, its geometry still sets tau_P).
+// kappa (per-element diffusivity, may be null = 1; no reference counterpart):
+// volume kappa_k grad u.grad v, face averages (kappa_M Dn_M + kappa_P Dn_P)/2,
+// penalty weighted by kappa_F = (kappa_M + kappa_P)/2 (kappa_M on Dirichlet
+// faces).  With kappa null every product by kappa is skipped, so the
+// reference operator is reproduced bit for bit.
 template <int N, typename T, bool USE_NBR, class NbrSrc>
 __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<N>::Np], const Geo<T>& g,
                                            const uint32_t (&w)[3], const T* __restrict__ geo, int ldg, T tau,
-                                           T alpha, const NbrSrc& nbr) {
+                                           T alpha, const NbrSrc& nbr, const T* __restrict__ kappa = nullptr,
+                                           int k = 0) {
   constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
   const RefMats<N, T>& R = CRef<N, T>::get();
+  const T kM = kappa ? __ldg(kappa + k) : T(1);
 
   // physical gradient at the nodes
   T ux[Np], uy[Np];
@@ -303,8 +310,8 @@ __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<
       a = fma(R.M[j * Np + i], ux[j], a);
       b = fma(R.M[j * Np + i], uy[j], b);
     }
-    ex[i] = g.J * a;
-    ey[i] = g.J * b;
+    ex[i] = kM * g.J * a;
+    ey[i] = kM * g.J * b;
   }
   // mass term (Helmholtz): alpha J (M u)
 #pragma unroll
@@ -331,9 +338,11 @@ __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<
     const T tauM = tau * sJ / g.J;
     T uP[Nfp], dnP[Nfp];
     T tauP = tauM;
+    T kP = kM;
     if (pact || mint) {
       const int kp = (int)(wf >> 7), fp = (int)(wf & 3);
       const bool flip = (wf >> 2) & 1;
+      if (kappa) kP = __ldg(kappa + kp);
       const T rxn = __ldg(geo + G_RX * ldg + kp), sxn = __ldg(geo + G_SX * ldg + kp);
       const T ryn = __ldg(geo + G_RY * ldg + kp), syn = __ldg(geo + G_SY * ldg + kp);
       const T Jn = __ldg(geo + G_J * ldg + kp);
@@ -375,20 +384,21 @@ __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<
         dnP[p] = T(0);
       }
     }
-    // coefficients
+    // coefficients (kappa_F: penalty weight of an interior face)
+    const T kF = kappa ? T(0.5) * (kM + kP) : T(1);
     const T caM = mdir ? T(1) : (mint ? T(0.5) : T(0));
-    const T cjM = mdir ? tauM : (mint ? T(0.5) * tauM : T(0));
-    const T cgM = mdir ? T(1) : (mint ? T(0.25) : T(0));
+    const T cjM = mdir ? (kappa ? tauM * kM : tauM) : (mint ? (kappa ? T(0.5) * tauM * kF : T(0.5) * tauM) : T(0));
+    const T cgM = (mdir ? T(1) : (mint ? T(0.25) : T(0))) * kM;
     const T caP = pact ? T(0.5) : T(0);
-    const T cjP = pact ? T(0.5) * tauP : T(0);
-    const T cgP = pact ? T(0.25) : T(0);
+    const T cjP = pact ? (kappa ? T(0.5) * tauP * kF : T(0.5) * tauP) : T(0);
+    const T cgP = (pact ? T(0.25) : T(0)) * kM;
     T v1[Nfp], v2[Nfp];
 #pragma unroll
     for (int p = 0; p < Nfp; ++p) {
       const T uM = u[fmask_idx(N, f, p)];
-      const T avgI = T(0.5) * (dnm[f][p] + dnP[p]);
+      const T avgI = kappa ? T(0.5) * (kM * dnm[f][p] + kP * dnP[p]) : T(0.5) * (dnm[f][p] + dnP[p]);
       const T jmpI = uM - uP[p];
-      const T avgM = mdir ? dnm[f][p] : avgI;
+      const T avgM = mdir ? (kappa ? kM * dnm[f][p] : dnm[f][p]) : avgI;
       const T jmpM = mdir ? uM : jmpI;
       v1[p] = -caM * avgM + cjM * jmpM - caP * avgI + cjP * jmpI;
       v2[p] = cgM * jmpM + cgP * jmpI;

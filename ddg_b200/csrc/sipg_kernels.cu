@@ -105,10 +105,10 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
     const Geo<T> g = load_geo(a.geo, a.ldg, k);
     if (MODE == AM_PFUSE) {
       NbrPfuse<T, Np> src{a.in0, a.in1, zc, beta, s_perm};
-      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src);
+      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src, a.kappa, k);
     } else {
       NbrPlain<T, Np> src{a.in0, s_perm};
-      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src);
+      elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src, a.kappa, k);
     }
     if (a.shift != 0.0) {
 #pragma unroll
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(BLOCK) k_self_blocks(BlockArgs a) {
     double u[Np], y[Np];
 #pragma unroll
     for (int i = 0; i < Np; ++i) u[i] = (i == j) ? 1.0 : 0.0;
-    elem_apply<N, double, false>(u, y, g, w, a.geo, a.ldg, a.tau, al, src);
+    elem_apply<N, double, false>(u, y, g, w, a.geo, a.ldg, a.tau, al, src, a.kappa, k);
 #pragma unroll
     for (int i = 0; i < Np; ++i) a.blocks[(size_t)kl * Np * Np + i * Np + j] = y[i] + (i == j ? a.shift : 0.0);
   }
@@ -530,6 +530,135 @@ __global__ void __launch_bounds__(BLOCK) k_cast_norm(int64_t n, const double* __
 __global__ void k_axpy_mixed(int64_t n, const float* __restrict__ x32, double* __restrict__ x64) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x64[i] += (double)x32[i];
+}
+
+// ================================================= kappa gradient (adjoint)
+// g_k = d a(u, lam; kappa) / d kappa_k: the volume term of element k plus,
+// per face, the derivative of the kappa-weighted average and penalty terms
+// (own side and, through the neighbour's half of an interior face, the
+// neighbour side).  Only the neighbours' traces are needed.
+template <int N, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_grad_kappa(GradArgs a) {
+  constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
+  __shared__ int s_perm[3 * Np];
+  for (int i = threadIdx.x; i < 3 * Np; i += BLOCK) s_perm[i] = a.perm[i];
+  __syncthreads();
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k >= a.K) return;
+  const RefMats<N, double>& R = CRef<N, double>::get();
+  const Geo<double> g = load_geo(a.geo, a.ldg, k);
+  double u[Np], l[Np], ux[Np], uy[Np], lx[Np], ly[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    u[i] = a.u[(size_t)k * Np + i];
+    l[i] = a.lam[(size_t)k * Np + i];
+  }
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    double ur = 0, us = 0, lr = 0, ls = 0;
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      ur = fma(R.Dr[i * Np + j], u[j], ur);
+      us = fma(R.Ds[i * Np + j], u[j], us);
+      lr = fma(R.Dr[i * Np + j], l[j], lr);
+      ls = fma(R.Ds[i * Np + j], l[j], ls);
+    }
+    ux[i] = g.rx * ur + g.sx * us;
+    uy[i] = g.ry * ur + g.sy * us;
+    lx[i] = g.rx * lr + g.sx * ls;
+    ly[i] = g.ry * lr + g.sy * ls;
+  }
+  double acc = 0.0;   // volume: J ux.(M lx) + uy.(M ly)   (sipg.py:189 with v = lam)
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    double mx = 0, my = 0;
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      mx = fma(R.M[i * Np + j], lx[j], mx);
+      my = fma(R.M[i * Np + j], ly[j], my);
+    }
+    acc += ux[i] * mx + uy[i] * my;
+  }
+  acc *= g.J;
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const uint32_t wf = __ldg(a.nbr + (size_t)f * a.K + k);
+    const int bc = (wf >> 3) & 3;
+    const bool pact = (wf >> 5) & 1, mint = (wf >> 6) & 1, mdir = (bc == 1);
+    if (!(pact || mint || mdir)) continue;
+    const double sJ = g.sJ[f], nx = g.nx[f], ny = g.ny[f];
+    const double tauM = a.tau * sJ / g.J;
+    double uM[Nfp], lM[Nfp], dU[Nfp], dL[Nfp], uP[Nfp], lP[Nfp];
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const int n = fmask_idx(N, f, p);
+      uM[p] = u[n];
+      lM[p] = l[n];
+      dU[p] = nx * ux[n] + ny * uy[n];
+      dL[p] = nx * lx[n] + ny * ly[n];
+      uP[p] = lP[p] = 0.0;
+    }
+    double tauP = tauM;
+    if (pact || mint) {
+      const int kp = (int)(wf >> 7), fp = (int)(wf & 3);
+      const bool flip = (wf >> 2) & 1;
+      tauP = a.tau * sJ / __ldg(a.geo + G_J * a.ldg + kp);
+      double ut[Nfp], lt[Nfp];
+#pragma unroll
+      for (int q = 0; q < Nfp; ++q) {
+        const size_t o = (size_t)kp * Np + s_perm[fp * Np + q];
+        ut[q] = __ldg(a.u + o);
+        lt[q] = __ldg(a.lam + o);
+      }
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) {
+        uP[p] = flip ? ut[N - p] : ut[p];
+        lP[p] = flip ? lt[N - p] : lt[p];
+      }
+    }
+    // weights: Dirichlet own side 1 (jumps against zero), interior halves 1/4
+    const double cA = mdir ? 1.0 : (mint ? 0.25 : 0.0) + (pact ? 0.25 : 0.0);
+    const double cT = mdir ? tauM : (mint ? 0.25 * tauM : 0.0) + (pact ? 0.25 * tauP : 0.0);
+    const double* m1 = R.m1d + f * Nfp * Nfp;
+    double face = 0.0;
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const double jU = mdir ? uM[p] : uM[p] - uP[p];
+#pragma unroll
+      for (int q = 0; q < Nfp; ++q) {
+        const double jL = mdir ? lM[q] : lM[q] - lP[q];
+        face += m1[p * Nfp + q] * (-cA * (dU[p] * jL + jU * dL[q]) + cT * jU * jL);
+      }
+    }
+    if (mdir && pact) {   // neighbour's interior half across a Dirichlet-tagged face
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p)
+#pragma unroll
+        for (int q = 0; q < Nfp; ++q) {
+          const double jU = uM[p] - uP[p], jL = lM[q] - lP[q];
+          face += m1[p * Nfp + q] * (-0.25 * (dU[p] * jL + jU * dL[q]) + 0.25 * tauP * jU * jL);
+        }
+    }
+    acc += sJ * face;
+  }
+  a.g[k] = acc;
+}
+
+template <int N>
+static cudaError_t launch_grad_n(const GradArgs& a, cudaStream_t s) {
+  constexpr int B = 128;
+  k_grad_kappa<N, B><<<(a.K + B - 1) / B, B, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_grad_kappa(int N, const GradArgs& a, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_grad_n<1>(a, s);
+    case 2: return launch_grad_n<2>(a, s);
+    case 3: return launch_grad_n<3>(a, s);
+    case 4: return launch_grad_n<4>(a, s);
+    case 5: return launch_grad_n<5>(a, s);
+  }
+  return cudaErrorInvalidValue;
 }
 
 // ============================================================ vectors

@@ -31,6 +31,7 @@ struct ApplyArgs {
   const T* binv;            // SMOOTH: packed block-Jacobi inverses (SoA)
   int ldb;
   double omega;             // SMOOTH: damping
+  const T* kappa;           // per-element diffusivity (null: 1)
 };
 
 template <typename T>
@@ -66,6 +67,19 @@ struct BlockArgs {
   int k0;             // first element
   int nbr_ld;         // element stride of the neighbour words (0: K)
   const double* alpha_e;  // per-element alpha (overrides alpha when set)
+  const double* kappa;    // per-element diffusivity (null: 1)
+};
+
+struct GradArgs {
+  const double* geo;
+  const uint32_t* nbr;
+  const int* perm;
+  const double* u;
+  const double* lam;
+  const double* kappa;    // unused by the contraction (a is linear in kappa)
+  double* g;              // out: d a(u, lam) / d kappa_k
+  int K, ldg;
+  double tau;
 };
 
 // Continuous-batching pool: per-request CG state on the device.
@@ -109,6 +123,7 @@ cudaError_t launch_block_jacobi(int N, const BlockArgs& a, cudaStream_t s);
 template <typename T>
 cudaError_t launch_pc_apply(int N, const T* r, T* z, const T* binv, int ldb, int K, cudaStream_t s);
 cudaError_t launch_rhs(int N, const RhsArgs& a, cudaStream_t s);
+cudaError_t launch_grad_kappa(int N, const GradArgs& a, cudaStream_t s);
 cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, double* y, cudaStream_t s);
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s);
 // r32 = float(r64), x32 = 0, ctl->bb = r32.r32 (reliable-update restart)

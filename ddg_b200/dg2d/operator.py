@@ -120,6 +120,27 @@ class SipgOperator:
                                            out.data_ptr(), _lib.stream_handle(stream)), "ddg_sipg_rhs")
         return out
 
+    # -- per-element diffusivity (extension) ------------------------------------
+    def set_kappa(self, kappa):
+        """Set (K positive values) or clear (None) the per-element diffusivity;
+        the block-Jacobi preconditioner must be rebuilt afterwards."""
+        if kappa is None:
+            _lib.check(_lib.lib().ddg_sipg_set_kappa(self._h, None), "ddg_sipg_set_kappa")
+        else:
+            k = np.ascontiguousarray(np.asarray(kappa, dtype=np.float64).reshape(-1))
+            if k.size != self.K:
+                raise ValueError(f"kappa needs {self.K} entries")
+            _lib.check(_lib.lib().ddg_sipg_set_kappa(self._h, k.ctypes.data), "ddg_sipg_set_kappa")
+        self.pc_alpha = None
+
+    def grad_kappa(self, u, lam, stream=None):
+        """g_k = d a(u, lam; kappa) / d kappa_k (float64 device vectors)."""
+        import torch
+        g = torch.empty(self.K, dtype=torch.float64, device=self._dev())
+        _lib.check(_lib.lib().ddg_sipg_grad_kappa(self._h, u.data_ptr(), lam.data_ptr(), g.data_ptr(),
+                                                  _lib.stream_handle(stream)), "ddg_sipg_grad_kappa")
+        return g
+
     # -- block Jacobi ----------------------------------------------------------
     def pc_build(self, alpha: float = 0.0, stream=None):
         _lib.check(_lib.lib().ddg_sipg_pc_build(self._h, float(alpha), _lib.stream_handle(stream)),

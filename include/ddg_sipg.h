@@ -171,6 +171,21 @@ int ddg_sipg_cg(ddg_sipg_op *op, const ddg_cg_config *cfg, const void *b,
 int ddg_sipg_cg_mixed(ddg_sipg_op *op, const ddg_cg_config *cfg, double delta,
                       const double *b, double *x, void *stream, ddg_solve_info *info);
 
+/* ---- per-element diffusivity and its adjoint gradient ------------------- */
+/* Extension with no reference counterpart (ddg's SIPG form has no
+ * coefficient): set (kappa: K host doubles > 0) or clear (NULL) a
+ * per-element diffusivity.  The operator becomes volume kappa_k grad u.grad v,
+ * face averages (kappa_M Dn_M + kappa_P Dn_P)/2 and penalty weight
+ * (kappa_M + kappa_P)/2 (kappa_M on Dirichlet faces); symmetric, and equal to
+ * the reference operator for kappa = 1.  Applies, CG (all precisions) and
+ * the block-Jacobi preconditioner use it (rebuild the preconditioner after
+ * setting it); multigrid and non-homogeneous Dirichlet loads do not. */
+int ddg_sipg_set_kappa(ddg_sipg_op *op, const double *kappa);
+/* g[k] = d a(u, lam; kappa) / d kappa_k for device float64 vectors u, lam;
+ * the kappa-gradient contraction of the adjoint method: with A u = b and
+ * A lam = dL/du, dL/dkappa = -g (a is linear in kappa). */
+int ddg_sipg_grad_kappa(ddg_sipg_op *op, const double *u, const double *lam, double *g, void *stream);
+
 /* ---- p / hp multigrid (src/ddg/dg2d/multigrid.py) ---------------------- */
 typedef struct ddg_mg ddg_mg;                /* opaque, library-owned */
 

@@ -75,11 +75,17 @@ def _unface(mesh, a):
 
 # ----------------------------------------------------- the operator -------
 
-def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
+def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
     """Explicit ``sipg_apply_2d`` (``sipg.py:304-337``): d a(u, v) / d v at
     v = 0, including the affine Dirichlet offset when ``u_dir`` is given.
 
     ``u`` is (Np, K) or (Np, K, B); the result has the same shape.
+
+    ``kappa`` (K,) is the per-element diffusivity extension (no reference
+    counterpart): volume kappa_k grad u . grad v, face averages
+    {kappa grad u . n} = (kappa_M Dn_M + kappa_P Dn_P)/2, penalty weighted by
+    kappa_F = (kappa_M + kappa_P)/2 (kappa_M on boundary faces).  kappa = 1
+    is the reference operator.
     """
     squeeze = u.ndim == 2
     ref = mesh.ref
@@ -89,6 +95,8 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
     M, m1d = ref.M, ref.m1d
     Dr, Ds = ref.Dr, ref.Ds
     rx, sx, ry, sy, J = (a[:, :, None] for a in (mesh.rx, mesh.sx, mesh.ry, mesh.sy, mesh.J))
+    kap = np.ones(K) if kappa is None else np.asarray(kappa, dtype=np.float64)
+    kvol = kap[None, :, None]
 
     ur = np.einsum("ij,jkb->ikb", Dr, U)
     us = np.einsum("ij,jkb->ikb", Ds, U)
@@ -96,8 +104,8 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
     uy = ry * ur + sy * us
 
     # volume term sum J*(ux*(M vx) + uy*(M vy))  (sipg.py:189)
-    cx = np.einsum("ji,jkb->ikb", M, J * ux)            # M^T (J ux)
-    cy = np.einsum("ji,jkb->ikb", M, J * uy)
+    cx = np.einsum("ji,jkb->ikb", M, kvol * J * ux)     # M^T (kappa J ux)
+    cy = np.einsum("ji,jkb->ikb", M, kvol * J * uy)
     gx = cx.copy()                                       # dL/dvx (per node)
     gy = cy.copy()
 
@@ -118,16 +126,19 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
         uPd = np.broadcast_to(uPd, uM.shape)
     uPeff = np.where(isd, uPd, np.where(isn, uM, uPraw))
     DnPeff = np.where(isb, DnM, DnPraw)
-    avg = 0.5 * (DnM + DnPeff)
+    kM = kap[vM // Np][:, None]
+    kP = np.where(isb, kM, kap[vP // Np][:, None])
+    avg = 0.5 * (kM * DnM + kP * DnPeff)
     jmp = uM - uPeff
+    kF = _face(mesh, (0.5 * (kM + kP))[:, 0])                         # (Nfp,3,K)
 
     sJ1 = _face(mesh, mesh.sJ.reshape(-1, order="F"))[0]             # (3, K)
     Fs1 = _face(mesh, mesh.Fscale.reshape(-1, order="F"))[0]
     tau = tau_scale * (mesh.N + 1) * (mesh.N + 1) * Fs1
     avgF, jmpF = _face(mesh, avg), _face(mesh, jmp)                   # (Nfp,3,K,B)
     wsJ = (w * sJ1)[None, :, :, None]
-    wtsJ = (w * tau * sJ1)[None, :, :, None]
-    # d/d(jmp_v): -w sJ m1d^T avg + w tau sJ m1d^T jmp   (sipg.py:270-279)
+    wtsJ = (w * tau * sJ1)[None, :, :, None] * kF[0][None, :, :, None]
+    # d/d(jmp_v): -w sJ m1d^T avg + w tau kappa_F sJ m1d^T jmp   (sipg.py:270-279)
     dj = (-wsJ * np.einsum("fpq,pfkb->qfkb", m1d, avgF)
           + wtsJ * np.einsum("fpq,pfkb->qfkb", m1d, jmpF))
     # d/d(avg_v): -w sJ m1d^T jmp_u
@@ -142,11 +153,11 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
     np.add.at(yf, vM, np.where(isn, 0.0, dj))
     np.add.at(yf, vP[isi], -dj[isi])
     # avg_v = 0.5 (Dn_vM + Dn_vPeff), Dn_vPeff = Dn_vM on boundary faces
-    cM = np.where(isb, 1.0, 0.5)
+    cM = np.where(isb, 1.0, 0.5) * kM
     np.add.at(gxf, vM, cM * nxf * da)
     np.add.at(gyf, vM, cM * nyf * da)
-    np.add.at(gxf, vP[isi], 0.5 * nxf[isi] * da[isi])
-    np.add.at(gyf, vP[isi], 0.5 * nyf[isi] * da[isi])
+    np.add.at(gxf, vP[isi], 0.5 * kP[isi] * nxf[isi] * da[isi])
+    np.add.at(gyf, vP[isi], 0.5 * kP[isi] * nyf[isi] * da[isi])
 
     gx = gx + _unflat(gxf, Np, K)
     gy = gy + _unflat(gyf, Np, K)
@@ -156,9 +167,11 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
     return y[:, :, 0] if squeeze else y
 
 
-def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0):
+def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
     """Literal restatement of ``sipg_bilinear_form`` (``sipg.py:142-301``,
-    affine ``cub=None`` branch) on torch float64 tensors."""
+    affine ``cub=None`` branch) on torch float64 tensors; ``kappa`` (a (K,)
+    tensor, may require grad) adds the diffusivity extension described in
+    :func:`apply` (kappa = 1 is the reference form)."""
     import torch
     ref = mesh.ref
     T = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float64)  # noqa: E731
@@ -169,7 +182,8 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0):
     uy = ry * (Dr @ u) + sy * (Ds @ u)
     vx = rx * (Dr @ v) + sx * (Ds @ v)
     vy = ry * (Dr @ v) + sy * (Ds @ v)
-    vol = torch.sum(J * (ux * (M @ vx) + uy * (M @ vy)))
+    kap = torch.ones(K, dtype=torch.float64) if kappa is None else kappa
+    vol = torch.sum(kap[None, :] * J * (ux * (M @ vx) + uy * (M @ vy)))
     fl = lambda a: a.T.reshape(-1)  # noqa: E731
     vM, vP = torch.as_tensor(mesh.vmapM), torch.as_tensor(mesh.vmapP)
     nx = T(mesh.nx.reshape(-1, order="F"))
@@ -184,14 +198,17 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0):
     isd = torch.as_tensor(bcn == BC_DIRICHLET)
     isn = torch.as_tensor(bcn == BC_NEUMANN)
     isb = isd | isn
+    tf = lambda a: a.reshape(K, 3, Nfp).permute(2, 1, 0)  # noqa: E731  (Nfp,3,K)
     uPd = torch.zeros_like(u_M) if u_dir is None else fl(T(u_dir))[vM]
     vPd = torch.zeros_like(v_M)
     uPe = torch.where(isd, uPd, torch.where(isn, u_M, u_P))
     vPe = torch.where(isd, vPd, torch.where(isn, v_M, v_P))
-    aDu = 0.5 * (DuM + torch.where(isb, DuM, DuP))
-    aDv = 0.5 * (DvM + torch.where(isb, DvM, DvP))
+    kM = kap[vM // Np]
+    kP = torch.where(isb, kM, kap[vP // Np])
+    aDu = 0.5 * (kM * DuM + kP * torch.where(isb, DuM, DuP))
+    aDv = 0.5 * (kM * DvM + kP * torch.where(isb, DvM, DvP))
+    kF = tf(0.5 * (kM + kP))[0]                                       # (3, K)
     ju, jv = u_M - uPe, v_M - vPe
-    tf = lambda a: a.reshape(K, 3, Nfp).permute(2, 1, 0)  # noqa: E731  (Nfp,3,K)
     sJ1 = T(mesh.sJ.reshape((Nfp, 3, K), order="F")[0])
     Fs1 = T(mesh.Fscale.reshape((Nfp, 3, K), order="F")[0])
     tau = tau_scale * (mesh.N + 1) * (mesh.N + 1) * Fs1
@@ -199,18 +216,35 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0):
     wsJ = wt * sJ1
     cons = -torch.einsum("fk,pfk,fpq,qfk->", wsJ, tf(aDu), m1d, tf(jv))
     adj = -torch.einsum("fk,pfk,fpq,qfk->", wsJ, tf(ju), m1d, tf(aDv))
-    pen = torch.einsum("fk,pfk,fpq,qfk->", wt * tau * sJ1, tf(ju), m1d, tf(jv))
+    pen = torch.einsum("fk,pfk,fpq,qfk->", wt * tau * sJ1 * kF, tf(ju), m1d, tf(jv))
     return vol + cons + adj + pen
 
 
-def apply_autograd(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0):
+def apply_autograd(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
     """``sipg_apply_2d`` exactly as the reference computes it: the gradient
     of the scalar form w.r.t. v at v = 0 (``sipg.py:329-337``)."""
     import torch
     ut = torch.as_tensor(np.asarray(u), dtype=torch.float64)
     v = torch.zeros_like(ut, requires_grad=True)
-    a = bilinear_form_torch(mesh, ut, v, bc_types=bc_types, u_dir=u_dir, tau_scale=tau_scale)
+    kt = None if kappa is None else torch.as_tensor(np.asarray(kappa), dtype=torch.float64)
+    a = bilinear_form_torch(mesh, ut, v, bc_types=bc_types, u_dir=u_dir, tau_scale=tau_scale, kappa=kt)
     (g,) = torch.autograd.grad(a, v)
+    return g.numpy()
+
+
+def grad_kappa(mesh, u, lam, *, bc_types, tau_scale=200.0, kappa=None):
+    """d a(u, lam; kappa) / d kappa_k per element, by torch autograd of the
+    literal form (a is linear in kappa, so this is exact).  With u the
+    solution of A(kappa) u = b and lam the adjoint A lam = dL/du, the loss
+    gradient is dL/dkappa = -grad_kappa(u, lam)."""
+    import torch
+    K = mesh.K
+    kt = torch.as_tensor(np.ones(K) if kappa is None else np.asarray(kappa), dtype=torch.float64)
+    kt.requires_grad_(True)
+    a = bilinear_form_torch(mesh, torch.as_tensor(np.asarray(u), dtype=torch.float64),
+                            torch.as_tensor(np.asarray(lam), dtype=torch.float64),
+                            bc_types=bc_types, tau_scale=tau_scale, kappa=kt)
+    (g,) = torch.autograd.grad(a, kt)
     return g.numpy()
 
 
@@ -221,7 +255,7 @@ def mass_apply(mesh, u):
     return mesh.J * (mesh.ref.M @ u)
 
 
-def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0):
+def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, kappa=None):
     """Matvec on the element-major flat vector; ``alpha M + A`` (alpha=0:
     ``sipg.py:876-883``; alpha>0: ``sipg.py:589-601`` and
     ``multigrid.py:53-74``).  Accepts (n,) or (n, B)."""
@@ -230,7 +264,7 @@ def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0):
     def op(x):
         X = x[:, None] if x.ndim == 1 else x
         U = _unflat(X, Np, K)
-        Y = apply(mesh, U, bc_types=bc_types, tau_scale=tau_scale)
+        Y = apply(mesh, U, bc_types=bc_types, tau_scale=tau_scale, kappa=kappa)
         if alpha != 0.0:
             Y = Y + alpha * mass_apply(mesh, U)
         out = _flat(Y)
@@ -238,11 +272,11 @@ def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0):
     return op
 
 
-def dense_matrix(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, chunk=512):
+def dense_matrix(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, chunk=512, kappa=None):
     """``sipg_matrix_2d`` (``sipg.py:344-364``) / ``sipg_helmholtz_matrix_2d``
     (``:460-496``; ``nu`` unused there too): columns of the apply."""
     n = mesh.Np * mesh.K
-    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha)
+    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha, kappa=kappa)
     A = np.zeros((n, n))
     for c0 in range(0, n, chunk):
         c1 = min(n, c0 + chunk)
