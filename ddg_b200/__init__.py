@@ -6,3 +6,14 @@ apply, Krylov iteration, preconditioner and load runs in the CUDA library
 """
 
 __version__ = "0.1.0"
+
+
+def pinned_empty(shape, dtype="float64"):
+    """A numpy array in page-locked host memory (a view of a pinned torch
+    tensor, kept alive by the array).  Host fields in pinned memory are
+    read and written by the GPU copy engines directly, e.g. by
+    ``SipgOperator.apply_host``."""
+    import numpy as np
+    import torch
+    t = torch.empty(tuple(shape), dtype=getattr(torch, np.dtype(dtype).name), pin_memory=True)
+    return t.numpy()

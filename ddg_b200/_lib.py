@@ -68,6 +68,7 @@ _PROTOS = {
     "ddg_sipg_destroy": (C.c_int, [_vp]),
     "ddg_sipg_set_bc": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "ddg_sipg_apply": (C.c_int, [_vp, C.c_int, C.c_double, _vp, _vp, _vp]),
+    "ddg_sipg_apply_host": (C.c_int, [_vp, C.c_double, _vp, _vp, _vp]),
     "ddg_sipg_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "ddg_sipg_pc_build": (C.c_int, [_vp, C.c_double, _vp]),
     "ddg_sipg_pc_apply": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),

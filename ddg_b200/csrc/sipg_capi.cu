@@ -73,6 +73,24 @@ struct CgGraph {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// State of the host-buffer apply (ddg_sipg_apply_host), created on first use:
+// node-major device copies of u and y, pinned staging for pageable host
+// arrays, one stream per direction plus one for the kernels, and per-chunk
+// events.  need[c] is the last element chunk whose values chunk c's
+// elements read through a face (neighbours), so chunk c's kernel waits only
+// for the host->device copies up to need[c].
+struct HostIO {
+  double* d_u = nullptr;
+  double* d_y = nullptr;
+  double* h_u = nullptr;   // pinned staging (pageable input)
+  double* h_y = nullptr;   // pinned staging (pageable output)
+  cudaStream_t s_in = nullptr, s_cmp = nullptr, s_out = nullptr;
+  cudaEvent_t e_start = nullptr;
+  std::vector<cudaEvent_t> e_in, e_cmp, e_out;
+  std::vector<int> need;
+  int nch = 0, chunk = 0;
+};
+
 }  // namespace
 
 struct ddg_sipg_op {
@@ -106,6 +124,7 @@ struct ddg_sipg_op {
   std::vector<int64_t> EToE, EToF, vmapP;
   std::vector<int64_t> rot;         // (3, Np)
   std::vector<uint32_t> nbr_host;
+  HostIO* hio = nullptr;            // host-buffer apply state (lazy)
 };
 
 namespace {
@@ -301,6 +320,18 @@ void free_op(ddg_sipg_op* op) {
       if (p) cudaFree(p);
   }
   if (op->cap) cudaStreamDestroy(op->cap);
+  if (HostIO* h = op->hio) {
+    if (h->d_u) cudaFree(h->d_u);
+    if (h->d_y) cudaFree(h->d_y);
+    if (h->h_u) cudaFreeHost(h->h_u);
+    if (h->h_y) cudaFreeHost(h->h_y);
+    for (auto* v : {&h->e_in, &h->e_cmp, &h->e_out})
+      for (cudaEvent_t ev : *v) cudaEventDestroy(ev);
+    if (h->e_start) cudaEventDestroy(h->e_start);
+    for (cudaStream_t st : {h->s_in, h->s_cmp, h->s_out})
+      if (st) cudaStreamDestroy(st);
+    delete h;
+  }
   delete op;
 }
 
@@ -461,6 +492,7 @@ extern "C" int ddg_sipg_set_bc(ddg_sipg_op* op, const int32_t* bc) {
   if (rc != DDG_OK) return rc;
   CK(cudaMemcpy(op->nbr, op->nbr_host.data(), op->nbr_host.size() * 4, cudaMemcpyHostToDevice));
   op->pc_ready = false;
+  if (op->hio) op->hio->need.clear();
   return DDG_OK;
 }
 
@@ -488,6 +520,118 @@ extern "C" int ddg_sipg_apply(ddg_sipg_op* op, int prec, double alpha, const voi
     return fail(DDG_ERR_INVALID, "precision must be DDG_FP64 or DDG_FP32");
   }
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("apply launch: ") + cudaGetErrorString(e));
+  return DDG_OK;
+}
+
+namespace {
+
+// Lazily create the host-buffer apply state and (after a BC change) its
+// chunk dependency table.
+int hio_prepare(ddg_sipg_op* op) {
+  const int K = op->K;
+  if (!op->hio) {
+    HostIO* h = new HostIO();
+    op->hio = h;  // released by free_op even when set-up stops halfway
+    h->nch = std::max(1, std::min(16, K / 4096));
+    h->chunk = (K + h->nch - 1) / h->nch;
+    h->nch = (K + h->chunk - 1) / h->chunk;
+    const size_t bytes = (size_t)K * op->Np * sizeof(double);
+    CK(cudaMalloc((void**)&h->d_u, bytes));
+    CK(cudaMalloc((void**)&h->d_y, bytes));
+    CK(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->s_cmp, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->e_start, cudaEventDisableTiming));
+    for (auto* v : {&h->e_in, &h->e_cmp, &h->e_out}) {
+      v->assign(h->nch, nullptr);
+      for (cudaEvent_t& ev : *v) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+  }
+  HostIO* h = op->hio;
+  if (h->need.empty()) {
+    // chunk c reads the values of every element that shares a face with one
+    // of its elements (neighbour words with the own-interior or
+    // neighbour-side bit set); kernels launch in chunk order, so keep the
+    // running maximum
+    std::vector<int> need(h->nch);
+    for (int c = 0; c < h->nch; ++c) need[c] = c;
+    for (int f = 0; f < 3; ++f)
+      for (int k = 0; k < K; ++k) {
+        const uint32_t w = op->nbr_host[(size_t)f * K + k];
+        if (w & (32u | 64u)) {
+          const int c = k / h->chunk, cp = (int)(w >> 7) / h->chunk;
+          if (cp > need[c]) need[c] = cp;
+        }
+      }
+    for (int c = 1; c < h->nch; ++c) need[c] = std::max(need[c], need[c - 1]);
+    h->need.swap(need);
+  }
+  return DDG_OK;
+}
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes at{};
+  const cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* u, double* y, void* stream) {
+  if (!op || !u || !y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: null argument");
+  if ((const void*)u == (const void*)y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: u and y must not alias");
+  DevGuard guard(op->dev);
+  int rc = hio_prepare(op);
+  if (rc != DDG_OK) return rc;
+  HostIO* h = op->hio;
+  const int K = op->K, Np = op->Np;
+  const size_t pitch = (size_t)K * sizeof(double), bytes = pitch * Np;
+  const bool u_pin = host_pinned(u), y_pin = host_pinned(y);
+  if (!u_pin && !h->h_u) CK(cudaMallocHost((void**)&h->h_u, bytes));
+  if (!y_pin && !h->h_y) CK(cudaMallocHost((void**)&h->h_y, bytes));
+  cudaStream_t us = (cudaStream_t)stream;
+  CK(cudaEventRecord(h->e_start, us));
+  for (cudaStream_t st : {h->s_in, h->s_cmp, h->s_out}) CK(cudaStreamWaitEvent(st, h->e_start, 0));
+  ApplyArgs<double> a = apply_args<double>(op);
+  a.in0 = h->d_u;
+  a.out0 = h->d_y;
+  a.alpha = alpha;
+  const double* src = u_pin ? u : h->h_u;
+  double* dst = y_pin ? y : h->h_y;
+  int next = 0;
+  for (int c = 0; c < h->nch; ++c) {
+    const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
+    const size_t w = (size_t)(c1 - c0) * sizeof(double);
+    if (!u_pin)  // stage this chunk while the previous one is in flight
+      for (int i = 0; i < Np; ++i) std::memcpy(h->h_u + (size_t)i * K + c0, u + (size_t)i * K + c0, w);
+    CK(cudaMemcpy2DAsync(h->d_u + c0, pitch, src + c0, pitch, w, Np, cudaMemcpyHostToDevice, h->s_in));
+    CK(cudaEventRecord(h->e_in[c], h->s_in));
+    for (; next < h->nch && h->need[next] <= c; ++next) {
+      const int j0 = next * h->chunk, j1 = std::min(K, j0 + h->chunk);
+      CK(cudaStreamWaitEvent(h->s_cmp, h->e_in[c], 0));
+      const cudaError_t e = launch_apply_nm<double>(op->N, a, j0, j1, h->s_cmp);
+      if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("apply launch: ") + cudaGetErrorString(e));
+      CK(cudaEventRecord(h->e_cmp[next], h->s_cmp));
+      CK(cudaStreamWaitEvent(h->s_out, h->e_cmp[next], 0));
+      CK(cudaMemcpy2DAsync(dst + j0, pitch, h->d_y + j0, pitch, (size_t)(j1 - j0) * sizeof(double), Np,
+                           cudaMemcpyDeviceToHost, h->s_out));
+      CK(cudaEventRecord(h->e_out[next], h->s_out));
+    }
+  }
+  if (!y_pin) {
+    for (int j = 0; j < h->nch; ++j) {
+      const int j0 = j * h->chunk, j1 = std::min(K, j0 + h->chunk);
+      CK(cudaEventSynchronize(h->e_out[j]));
+      for (int i = 0; i < Np; ++i)
+        std::memcpy(y + (size_t)i * K + j0, h->h_y + (size_t)i * K + j0, (size_t)(j1 - j0) * sizeof(double));
+    }
+  } else {
+    CK(cudaStreamSynchronize(h->s_out));
+  }
   return DDG_OK;
 }
 

@@ -197,6 +197,52 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
   }
 }
 
+// ====================================================== node-major apply
+// y = A u + alpha J M u for the elements [k_begin, k_end) of fields stored
+// node-major, (Np, ld) row-major with ld = K: the reference's own (Np, K)
+// field layout (src/ddg/dg2d/sipg.py:304-337 takes and returns (Np, K)).
+// Thread k reads u[i * ld + k], so each warp load is one coalesced 256-byte
+// (float64) row segment and no shared-memory staging is needed.  Used by the
+// host-buffer entry point, which copies (Np, K) fields chunk by chunk and
+// launches this kernel per element chunk as soon as the chunk's neighbours
+// have arrived.
+template <typename T, int Np>
+struct NbrNodeMajor {
+  const T* __restrict__ u;
+  int ld;
+  const int* perm;  // shared memory, 3*Np
+  __device__ __forceinline__ void operator()(int kp, int fp, T (&ut)[Np]) const {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) ut[i] = __ldg(u + (size_t)perm[fp * Np + i] * ld + kp);
+  }
+};
+
+template <int N, typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_apply_nm(ApplyArgs<T> a, int k_begin, int k_end) {
+  constexpr int Np = Dim<N>::Np;
+  __shared__ int s_perm[3 * Np];
+  for (int i = threadIdx.x; i < 3 * Np; i += BLOCK) s_perm[i] = a.perm[i];
+  __syncthreads();
+  const int k = k_begin + blockIdx.x * BLOCK + threadIdx.x;
+  if (k >= k_end) return;
+  const int ld = a.K;
+  T u[Np], y[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) u[i] = __ldg(a.in0 + (size_t)i * ld + k);
+  uint32_t w[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) w[f] = __ldg(a.nbr + (size_t)f * a.K + k);
+  const Geo<T> g = load_geo(a.geo, a.ldg, k);
+  NbrNodeMajor<T, Np> src{a.in0, ld, s_perm};
+  elem_apply<N, T, true>(u, y, g, w, a.geo, a.ldg, T(a.tau), T(a.alpha), src, a.kappa, k);
+  if (a.shift != 0.0) {
+#pragma unroll
+    for (int i = 0; i < Np; ++i) y[i] += T(a.shift) * u[i];
+  }
+#pragma unroll
+  for (int i = 0; i < Np; ++i) a.out0[(size_t)i * ld + k] = y[i];
+}
+
 // ================================================================= CG
 // One CG step after the apply: x += alpha p; r -= alpha Ap; z = B^-1 r;
 // partials r.z, r.r -> last block: gamma, beta, iter, loop condition.
@@ -764,6 +810,28 @@ cudaError_t launch_apply(int N, int mode, const ApplyArgs<T>& a, cudaStream_t s)
 }
 template cudaError_t launch_apply<double>(int, int, const ApplyArgs<double>&, cudaStream_t);
 template cudaError_t launch_apply<float>(int, int, const ApplyArgs<float>&, cudaStream_t);
+
+template <int N, typename T>
+static cudaError_t launch_apply_nm_n(const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s) {
+  constexpr int B = 128;
+  const int n = k_end - k_begin;
+  if (n <= 0) return cudaSuccess;
+  k_apply_nm<N, T, B><<<(n + B - 1) / B, B, 0, s>>>(a, k_begin, k_end);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s) {
+  switch (N) {
+    case 1: return launch_apply_nm_n<1, T>(a, k_begin, k_end, s);
+    case 2: return launch_apply_nm_n<2, T>(a, k_begin, k_end, s);
+    case 3: return launch_apply_nm_n<3, T>(a, k_begin, k_end, s);
+    case 4: return launch_apply_nm_n<4, T>(a, k_begin, k_end, s);
+    case 5: return launch_apply_nm_n<5, T>(a, k_begin, k_end, s);
+  }
+  return cudaErrorInvalidValue;
+}
+template cudaError_t launch_apply_nm<double>(int, const ApplyArgs<double>&, int, int, cudaStream_t);
 
 int apply_grid(int K) { return (K + 127) / 128; }
 int cg_grid(int K) { return (K + 127) / 128; }

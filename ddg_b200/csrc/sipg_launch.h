@@ -117,6 +117,9 @@ struct RhsArgs {
 cudaError_t upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d);
 template <typename T>
 cudaError_t launch_apply(int N, int mode, const ApplyArgs<T>& a, cudaStream_t s);
+// node-major (Np, K) fields, elements [k_begin, k_end) only (in0 -> out0)
+template <typename T>
+cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s);
 template <typename T>
 cudaError_t launch_cg_step(int N, bool pc, bool init, const CgArgs<T>& a, cudaStream_t s);
 cudaError_t launch_block_jacobi(int N, const BlockArgs& a, cudaStream_t s);

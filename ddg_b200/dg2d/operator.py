@@ -109,6 +109,24 @@ class SipgOperator:
                                              y.data_ptr(), _lib.stream_handle(stream)), "ddg_sipg_apply")
         return y
 
+    def apply_host(self, u, *, alpha: float = 0.0, out=None, stream=None):
+        """y = A u + alpha J M u for a float64 HOST field of shape (Np, K)
+        (the reference's own field layout).  Copies, kernels and the copy
+        back overlap chunk by chunk inside the library; pinned arrays (see
+        :func:`ddg_b200.pinned_empty`) move at full copy-engine speed,
+        pageable ones are staged.  Returns ``out`` (allocated if None)."""
+        u = np.asarray(u)
+        if u.dtype != np.float64 or not u.flags.c_contiguous:
+            u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != (self.Np, self.K):
+            raise ValueError(f"u has shape {u.shape}, expected (Np, K) = {(self.Np, self.K)}")
+        y = np.empty((self.Np, self.K), dtype=np.float64) if out is None else out
+        if y.shape != (self.Np, self.K) or y.dtype != np.float64 or not y.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 (Np, K) array")
+        _lib.check(_lib.lib().ddg_sipg_apply_host(self._h, float(alpha), u.ctypes.data, y.ctypes.data,
+                                                  _lib.stream_handle(stream)), "ddg_sipg_apply_host")
+        return y
+
     def rhs(self, f=None, u_dir=None, q_neu=None, stream=None):
         """J M f - L_D(u_dir) + L_N(q_neu), float64 flat vectors (q_neu: face flat)."""
         import torch

@@ -111,6 +111,9 @@ def sipg_apply_2d(mesh: Mesh2D, u, *, bc_types, u_dir=None, tau_scale: float = 2
     element's own matrices."""
     _check_cub(cub)
     op = _op(mesh, bc_types, tau_scale)
+    if u_dir is None and not _is_torch(u):
+        # host (Np, K) arrays: chunked copy / apply / copy-back pipeline
+        return op.apply_host(u)
     dev = op._dev()
     y = op.apply(_flat(u, dev))
     if u_dir is not None:

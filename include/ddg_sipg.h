@@ -102,6 +102,20 @@ int ddg_sipg_set_bc(ddg_sipg_op *op, const int32_t *bc_types);
 int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
                    const void *u, void *y, void *stream);
 
+/* y = A u + alpha * J (M_ref u) for float64 HOST fields in the reference's
+ * own (Np, K) row-major layout: sipg_apply_2d(mesh, u, bc_types=...) of
+ * src/ddg/dg2d/sipg.py:304-337 as called with numpy arrays, which take and
+ * return (Np, K).  The call copies u to the device in element chunks on one
+ * stream, runs the apply of each chunk as soon as the chunks holding its
+ * face neighbours have arrived, and copies y back on a second stream, so the
+ * two transfer directions and the kernels overlap.  Pinned (page-locked)
+ * u / y are read / written directly by the copy engines; pageable ones are
+ * staged through the handle's pinned buffers (allocated on first use).
+ * Returns after y is complete; `stream`'s earlier work is ordered before
+ * the copies. */
+int ddg_sipg_apply_host(ddg_sipg_op *op, double alpha, const double *u, double *y,
+                        void *stream);
+
 /* rhs = J (M_ref f) - L_D(u_dir) + L_N(q_neu), all float64 device vectors.
  * Replaces the RHS assembly of src/ddg/dg2d/sipg.py:852-864 with
  * sipg_dirichlet_load_2d (:398-417) and sipg_neumann_load_2d (:420-453).
