@@ -18,6 +18,8 @@ DDG_FP32 = 1
 DDG_PC_NONE = 0
 DDG_PC_JACOBI = 1
 DDG_MAX_DEGREE = 5
+DDG_ENGINE_CUDA_CORES = 0
+DDG_ENGINE_TENSOR_CORES = 1
 SOLVE_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "device_error", 4: "stagnated"}
 
 
@@ -69,6 +71,7 @@ _PROTOS = {
     "ddg_sipg_set_bc": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "ddg_sipg_apply": (C.c_int, [_vp, C.c_int, C.c_double, _vp, _vp, _vp]),
     "ddg_sipg_apply_host": (C.c_int, [_vp, C.c_double, _vp, _vp, _vp]),
+    "ddg_sipg_set_engine": (C.c_int, [_vp, C.c_int]),
     "ddg_sipg_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "ddg_sipg_pc_build": (C.c_int, [_vp, C.c_double, _vp]),
     "ddg_sipg_pc_apply": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),

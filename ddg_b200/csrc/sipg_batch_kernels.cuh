@@ -59,13 +59,14 @@ __global__ void __launch_bounds__(BLOCK) k_batch_step(BatchArgs a, const double*
     a.r[o + i] = rv[i];
     rr += rv[i] * rv[i];
   }
+  {
+    double zv[Np];
+    sym_block_apply<Np, double>(a.binv + k, (size_t)a.cap, rv, zv);
 #pragma unroll
-  for (int i = 0; i < Np; ++i) {
-    double acc = 0.0;
-#pragma unroll
-    for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.cap + k), rv[j], acc);
-    a.z[o + i] = acc;
-    rz += rv[i] * acc;
+    for (int i = 0; i < Np; ++i) {
+      a.z[o + i] = zv[i];
+      rz += rv[i] * zv[i];
+    }
   }
   a.epA[k] = rz;
   a.epB[k] = rr;
@@ -143,13 +144,14 @@ __global__ void __launch_bounds__(BLOCK) k_batch_init(BatchArgs a, double* __res
     p0[o + i] = 0.0;
     rr += rv[i] * rv[i];
   }
+  {
+    double zv[Np];
+    sym_block_apply<Np, double>(a.binv + k, (size_t)a.cap, rv, zv);
 #pragma unroll
-  for (int i = 0; i < Np; ++i) {
-    double acc = 0.0;
-#pragma unroll
-    for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.cap + k), rv[j], acc);
-    a.z[o + i] = acc;
-    rz += rv[i] * acc;
+    for (int i = 0; i < Np; ++i) {
+      a.z[o + i] = zv[i];
+      rz += rv[i] * zv[i];
+    }
   }
   a.epA[k] = rz;
   a.epB[k] = rr;

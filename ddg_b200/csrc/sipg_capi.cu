@@ -59,7 +59,9 @@ struct Work {  // CG vectors of one precision (element-major, K*Np)
 struct GraphKey {
   int prec, pc;
   double alpha, shift;
+  int engine = 0;  // float32 apply engine captured in the graph
   bool operator<(const GraphKey& o) const {
+    if (engine != o.engine) return engine < o.engine;
     if (prec != o.prec) return prec < o.prec;
     if (pc != o.pc) return pc < o.pc;
     if (alpha != o.alpha) return alpha < o.alpha;
@@ -125,6 +127,8 @@ struct ddg_sipg_op {
   std::vector<int64_t> rot;         // (3, Np)
   std::vector<uint32_t> nbr_host;
   HostIO* hio = nullptr;            // host-buffer apply state (lazy)
+  uint8_t* tc_img = nullptr;        // tensor-core B operands of this degree (device)
+  int fp32_engine = DDG_ENGINE_TENSOR_CORES;
 };
 
 namespace {
@@ -257,7 +261,14 @@ int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGra
     a.in1 = (const T*)pin;
     a.out0 = (T*)w.Ap;
     a.out1 = (T*)pout;
-    e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+    if constexpr (sizeof(T) == 4) {
+      if (key.engine == DDG_ENGINE_TENSOR_CORES)
+        e = launch_apply_tc(op->N, AM_PFUSE, a, op->tc_img, op->cap);
+      else
+        e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+    } else {
+      e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+    }
     if (e != cudaSuccess) break;
     c.p = (const T*)pout;
     e = launch_cg_step<T>(op->N, key.pc != 0, false, c, op->cap);
@@ -310,6 +321,7 @@ void free_op(ddg_sipg_op* op) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
   }
+  if (op->tc_img) cudaFree(op->tc_img);
   void* ptrs[] = {op->kappa64, op->kappa32, op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
                   op->ticket, op->dotbuf, op->blocks, op->binv64, op->binv32};
   for (void* p : ptrs)
@@ -468,6 +480,14 @@ extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
   if (e == cudaSuccess) e = cudaMemset(op->ctl, 0, sizeof(CgCtl));
   if (e == cudaSuccess) e = cudaMemset(op->ticket, 0, sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess && tc_supported(N)) {
+    std::vector<uint8_t> img((size_t)tc_image_bytes(N), 0);
+    tc_build_image(N, d->Dr, d->Ds, d->M, img.data());
+    e = cudaMalloc((void**)&op->tc_img, img.size());
+    if (e == cudaSuccess) e = cudaMemcpy(op->tc_img, img.data(), img.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = tc_prepare(N);
+  }
+  if (!tc_supported(N)) op->fp32_engine = DDG_ENGINE_CUDA_CORES;
   if (e != cudaSuccess) {
     free_op(op);
     return fail(e == cudaErrorMemoryAllocation ? DDG_ERR_NOMEM : DDG_ERR_CUDA,
@@ -515,7 +535,10 @@ extern "C" int ddg_sipg_apply(ddg_sipg_op* op, int prec, double alpha, const voi
     a.out0 = (float*)y;
     a.alpha = alpha;
     a.use_tma = aligned16(u) && aligned16(y);
-    e = launch_apply<float>(op->N, AM_APPLY, a, s);
+    if (op->fp32_engine == DDG_ENGINE_TENSOR_CORES && op->tc_img && a.use_tma)
+      e = launch_apply_tc(op->N, AM_APPLY, a, op->tc_img, s);
+    else
+      e = launch_apply<float>(op->N, AM_APPLY, a, s);
   } else {
     return fail(DDG_ERR_INVALID, "precision must be DDG_FP64 or DDG_FP32");
   }
@@ -635,6 +658,21 @@ extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* 
   return DDG_OK;
 }
 
+extern "C" int ddg_sipg_set_engine(ddg_sipg_op* op, int engine) {
+  if (!op) return fail(DDG_ERR_INVALID, "ddg_sipg_set_engine: null handle");
+  if (engine == DDG_ENGINE_CUDA_CORES) {
+    op->fp32_engine = engine;
+    return DDG_OK;
+  }
+  if (engine == DDG_ENGINE_TENSOR_CORES) {
+    if (!op->tc_img)
+      return fail(DDG_ERR_UNSUPPORTED, "tensor-core float32 apply is built for degrees 1..4 only");
+    op->fp32_engine = engine;
+    return DDG_OK;
+  }
+  return fail(DDG_ERR_INVALID, "engine must be DDG_ENGINE_CUDA_CORES or DDG_ENGINE_TENSOR_CORES");
+}
+
 extern "C" int ddg_sipg_rhs(ddg_sipg_op* op, const double* f, const double* u_dir, const double* q_neu,
                             double* rhs, void* stream) {
   if (!op || !rhs) return fail(DDG_ERR_INVALID, "ddg_sipg_rhs: null argument");
@@ -730,6 +768,7 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
   Work& w = op->w[prec];
   cudaStream_t s = (cudaStream_t)stream;
   GraphKey key{prec, cfg->pc, cfg->alpha, cfg->shift};
+  key.engine = (prec == DDG_FP32 && op->tc_img) ? op->fp32_engine : DDG_ENGINE_CUDA_CORES;
   CgGraph* gr = nullptr;
   rc = get_graph(op, key, &gr);
   if (rc != DDG_OK) return rc;
@@ -872,6 +911,7 @@ extern "C" int ddg_sipg_cg_mixed(ddg_sipg_op* op, const ddg_cg_config* cfg, doub
   Work& w64 = op->w[DDG_FP64];
   Work& w32 = op->w[DDG_FP32];
   GraphKey key{DDG_FP32, cfg->pc, cfg->alpha, cfg->shift};
+  key.engine = op->tc_img ? op->fp32_engine : DDG_ENGINE_CUDA_CORES;
   CgGraph* gr = nullptr;
   rc = get_graph(op, key, &gr);
   if (rc != DDG_OK) return rc;

@@ -64,6 +64,24 @@ __host__ __device__ constexpr int sym_idx(int Np, int i, int j) {
   return i <= j ? i * Np - i * (i - 1) / 2 + (j - i) : j * Np - j * (j - 1) / 2 + (i - j);
 }
 
+// z = B^-1 r for one element from its packed symmetric inverse, stored
+// structure-of-arrays with stride ld (bk points at entry 0 of the element):
+// every entry is loaded once and used for (i, j) and (j, i).
+template <int Np, typename T>
+__device__ __forceinline__ void sym_block_apply(const T* __restrict__ bk, size_t ld, const T (&rv)[Np],
+                                                T (&zv)[Np]) {
+#pragma unroll
+  for (int i = 0; i < Np; ++i) zv[i] = T(0);
+#pragma unroll
+  for (int i = 0; i < Np; ++i)
+#pragma unroll
+    for (int j = i; j < Np; ++j) {
+      const T b = __ldg(bk + (size_t)sym_idx(Np, i, j) * ld);
+      zv[i] = fma(b, rv[j], zv[i]);
+      if (j != i) zv[j] = fma(b, rv[i], zv[j]);
+    }
+}
+
 // ---------------------------------------------------------------- layout
 // Geometry: structure-of-arrays geo[c * ldg + k].
 enum GeoField { G_RX = 0, G_SX, G_RY, G_SY, G_J, G_F0 = 5, G_COUNT = 14 };

@@ -4,6 +4,8 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "sipg_device.cuh"
 #include "sipg_launch.h"
@@ -129,21 +131,25 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
   }
   __syncthreads();  // every tile read done before the tiles are overwritten
   if (MODE == AM_SMOOTH) {
-    // residual of each element into tile 1, then x += omega B^-1 r with one
-    // (element, row) pair per thread (coalesced packed-inverse loads)
+    // x += omega B^-1 r for this thread's element: the residual is already in
+    // registers; each packed-symmetric entry of the inverse is loaded once
+    // (coalesced across the warp's elements) and used for (i, j) and (j, i)
     if (active) {
+      T zv[Np];
 #pragma unroll
-      for (int i = 0; i < Np; ++i) s_tile[1][tid * Np + i] = y[i];
-    }
-    __syncthreads();
-    const T om = T(a.omega);
-    for (int idx = tid; idx < nk * Np; idx += BLOCK) {
-      const int i = idx / nk, e = idx - i * nk;
-      const T* rv = s_tile[1] + e * Np;
-      T acc = T(0);
+      for (int i = 0; i < Np; ++i) zv[i] = T(0);
+      const T* bk = a.binv + k0 + tid;
 #pragma unroll
-      for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.ldb + k0 + e), rv[j], acc);
-      s_tile[0][e * Np + i] += om * acc;
+      for (int i = 0; i < Np; ++i)
+#pragma unroll
+        for (int j = i; j < Np; ++j) {
+          const T b = __ldg(bk + (size_t)sym_idx(Np, i, j) * a.ldb);
+          zv[i] = fma(b, y[j], zv[i]);
+          if (j != i) zv[j] = fma(b, y[i], zv[j]);
+        }
+      const T om = T(a.omega);
+#pragma unroll
+      for (int i = 0; i < Np; ++i) s_tile[0][tid * Np + i] += om * zv[i];
     }
   } else if (active) {
 #pragma unroll
@@ -251,8 +257,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply_nm(ApplyArgs<T> a, int k_begin,
 template <int N, typename T, bool PC, bool INIT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
   constexpr int Np = Dim<N>::Np;
-  __shared__ __align__(16) T s_r[BLOCK * Np];
-  __shared__ __align__(16) T s_z[PC ? BLOCK * Np : 1];
+  __shared__ __align__(16) T s_r[BLOCK * Np];  // r tile, then z tile (PC)
   __shared__ double s_red[64];
   if (!INIT && a.ctl->cont == 0) {
     // the loop already stopped: make sure the while node sees 0
@@ -280,20 +285,34 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
     if (PC) s_r[i] = rn;
   }
   if (PC) {
-    // z = B^-1 r, one (element, row) pair per thread: loads of the packed
-    // inverse are coalesced across the elements of a warp
+    // z = B^-1 r, one element per thread with the packed-symmetric indices
+    // known at compile time: each load of the inverse is one coalesced row
+    // segment across the warp's elements and each entry is loaded once
     __syncthreads();
-    for (int idx = tid; idx < nk * Np; idx += BLOCK) {
-      const int i = idx / nk, e = idx - i * nk;
-      const T* rv = s_r + e * Np;
-      T acc = T(0);
+    if (tid < nk) {
+      T rv[Np], zv[Np];
 #pragma unroll
-      for (int j = 0; j < Np; ++j) acc = fma(__ldg(a.binv + (size_t)sym_idx(Np, i, j) * a.ldb + k0 + e), rv[j], acc);
-      s_z[e * Np + i] = acc;
-      rz += (double)rv[i] * (double)acc;
+      for (int j = 0; j < Np; ++j) {
+        rv[j] = s_r[tid * Np + j];
+        zv[j] = T(0);
+      }
+      const T* bk = a.binv + k0 + tid;
+#pragma unroll
+      for (int i = 0; i < Np; ++i)
+#pragma unroll
+        for (int j = i; j < Np; ++j) {
+          const T b = __ldg(bk + (size_t)sym_idx(Np, i, j) * a.ldb);
+          zv[i] = fma(b, rv[j], zv[i]);
+          if (j != i) zv[j] = fma(b, rv[i], zv[j]);
+        }
+#pragma unroll
+      for (int i = 0; i < Np; ++i) {
+        s_r[tid * Np + i] = zv[i];  // own slots only: rv was read above
+        rz += (double)rv[i] * (double)zv[i];
+      }
     }
     __syncthreads();
-    for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_z[i];
+    for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_r[i];
   } else {
     rz = rr;
   }
@@ -443,16 +462,23 @@ __global__ void __launch_bounds__(BLOCK) k_pc_apply(const T* __restrict__ r, T* 
   __syncthreads();
   if (tid < nk) {
     const int k = k0 + tid;
-    T rv[Np];
+    T rv[Np], zv[Np];
 #pragma unroll
-    for (int j = 0; j < Np; ++j) rv[j] = s[tid * Np + j];
-#pragma unroll
-    for (int i = 0; i < Np; ++i) {
-      T acc = T(0);
-#pragma unroll
-      for (int j = 0; j < Np; ++j) acc = fma(__ldg(binv + (size_t)sym_idx(Np, i, j) * ldb + k), rv[j], acc);
-      s[tid * Np + i] = acc;
+    for (int j = 0; j < Np; ++j) {
+      rv[j] = s[tid * Np + j];
+      zv[j] = T(0);
     }
+    // each packed-symmetric entry loaded once, used for (i, j) and (j, i)
+#pragma unroll
+    for (int i = 0; i < Np; ++i)
+#pragma unroll
+      for (int j = i; j < Np; ++j) {
+        const T b = __ldg(binv + (size_t)sym_idx(Np, i, j) * ldb + k);
+        zv[i] = fma(b, rv[j], zv[i]);
+        if (j != i) zv[j] = fma(b, rv[i], zv[j]);
+      }
+#pragma unroll
+    for (int i = 0; i < Np; ++i) s[tid * Np + i] = zv[i];
   }
   __syncthreads();
   for (int i = tid; i < nk * Np; i += BLOCK) z[off + i] = s[i];
@@ -956,3 +982,4 @@ cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double
 }  // namespace ddg
 
 #include "sipg_batch_kernels.cuh"
+#include "sipg_tc.cuh"

@@ -117,6 +117,14 @@ struct RhsArgs {
 cudaError_t upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d);
 template <typename T>
 cudaError_t launch_apply(int N, int mode, const ApplyArgs<T>& a, cudaStream_t s);
+// float32 apply on the tensor cores (tcgen05, 3xTF32); `img` is the device
+// copy of the degree's B-operand image (tc_build_image)
+bool tc_supported(int N);
+int tc_image_bytes(int N);
+int tc_build_image(int N, const double* Dr, const double* Ds, const double* M, uint8_t* out);
+// modes AM_APPLY and AM_PFUSE; tc_prepare sets the kernels' attributes
+cudaError_t tc_prepare(int N);
+cudaError_t launch_apply_tc(int N, int mode, const ApplyArgs<float>& a, const uint8_t* img, cudaStream_t s);
 // node-major (Np, K) fields, elements [k_begin, k_end) only (in0 -> out0)
 template <typename T>
 cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s);

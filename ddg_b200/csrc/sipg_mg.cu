@@ -49,7 +49,8 @@ __global__ void k_dense_gemv(int n, const T* __restrict__ A, const T* __restrict
   if (lane == 0) x[warp] = (T)acc;
 }
 
-// x = scale * B^-1 b, one (element, row) pair per thread (packed inverses).
+// x = scale * B^-1 b, one element per thread (packed inverses: each entry
+// loaded once, coalesced across the warp's elements, used for (i,j), (j,i)).
 template <int N, typename T, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_bj_scaled(const T* __restrict__ b, T* __restrict__ x,
                                                      const T* __restrict__ binv, int ldb, int K, T scale) {
@@ -59,13 +60,27 @@ __global__ void __launch_bounds__(BLOCK) k_bj_scaled(const T* __restrict__ b, T*
   const size_t off = (size_t)k0 * Np;
   for (int i = tid; i < nk * Np; i += BLOCK) s[i] = b[off + i];
   __syncthreads();
-  for (int idx = tid; idx < nk * Np; idx += BLOCK) {
-    const int i = idx / nk, e = idx - i * nk;
-    T acc = T(0);
+  if (tid < nk) {
+    T rv[Np], zv[Np];
 #pragma unroll
-    for (int j = 0; j < Np; ++j) acc = fma(__ldg(binv + (size_t)sym_idx(Np, i, j) * ldb + k0 + e), s[e * Np + j], acc);
-    x[off + (size_t)e * Np + i] = scale * acc;
+    for (int j = 0; j < Np; ++j) {
+      rv[j] = s[tid * Np + j];
+      zv[j] = T(0);
+    }
+    const T* bk = binv + k0 + tid;
+#pragma unroll
+    for (int i = 0; i < Np; ++i)
+#pragma unroll
+      for (int j = i; j < Np; ++j) {
+        const T c = __ldg(bk + (size_t)sym_idx(Np, i, j) * ldb);
+        zv[i] = fma(c, rv[j], zv[i]);
+        if (j != i) zv[j] = fma(c, rv[i], zv[j]);
+      }
+#pragma unroll
+    for (int i = 0; i < Np; ++i) s[tid * Np + i] = scale * zv[i];
   }
+  __syncthreads();
+  for (int i = tid; i < nk * Np; i += BLOCK) x[off + i] = s[i];
 }
 
 // CG with an external preconditioner, part 1: x += alpha p, r -= alpha Ap,

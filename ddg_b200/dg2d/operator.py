@@ -127,6 +127,12 @@ class SipgOperator:
                                                   _lib.stream_handle(stream)), "ddg_sipg_apply_host")
         return y
 
+    def set_engine(self, engine: str):
+        """float32 apply engine: "tensor" (tcgen05, 3xTF32; degrees 1..4) or
+        "cuda" (plain float32 FMA)."""
+        code = {"tensor": _lib.DDG_ENGINE_TENSOR_CORES, "cuda": _lib.DDG_ENGINE_CUDA_CORES}[engine]
+        _lib.check(_lib.lib().ddg_sipg_set_engine(self._h, code), "ddg_sipg_set_engine")
+
     def rhs(self, f=None, u_dir=None, q_neu=None, stream=None):
         """J M f - L_D(u_dir) + L_N(q_neu), float64 flat vectors (q_neu: face flat)."""
         import torch

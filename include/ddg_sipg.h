@@ -102,6 +102,17 @@ int ddg_sipg_set_bc(ddg_sipg_op *op, const int32_t *bc_types);
 int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
                    const void *u, void *y, void *stream);
 
+/* Engine of the float32 operator apply (ddg_sipg_apply with DDG_FP32).
+ * DDG_ENGINE_TENSOR_CORES (default for degrees 1..4): the element
+ * contractions run on the tcgen05 tensor cores with 3xTF32 splitting
+ * (float32-accurate); DDG_ENGINE_CUDA_CORES: plain float32 FMA on the CUDA
+ * cores (the only engine for degree 5).  No reference counterpart (the
+ * reference computes in float64 only); used by the float32 applies of the
+ * mixed-precision solves. */
+#define DDG_ENGINE_CUDA_CORES   0
+#define DDG_ENGINE_TENSOR_CORES 1
+int ddg_sipg_set_engine(ddg_sipg_op *op, int engine);
+
 /* y = A u + alpha * J (M_ref u) for float64 HOST fields in the reference's
  * own (Np, K) row-major layout: sipg_apply_2d(mesh, u, bc_types=...) of
  * src/ddg/dg2d/sipg.py:304-337 as called with numpy arrays, which take and

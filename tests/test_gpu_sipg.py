@@ -331,3 +331,77 @@ def test_apply_host_chunked_pipeline(Kx, Ky, N, shuffle):
             got = op.apply_host(src, alpha=5.0, out=out)
             assert np.array_equal(got, dev)
     assert _rel(dev, ref) < APPLY_RTOL64
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4])
+@pytest.mark.parametrize("bcname", ["dirichlet", "neumann", "mixed"])
+def test_apply_fp32_tensor_cores_match_oracle(N, bcname):
+    """float32 apply on the tcgen05 tensor cores (3xTF32) vs the float64
+    oracle, and vs the CUDA-core float32 engine; a mesh whose element count
+    is not a multiple of the 128-element tile exercises the partial tile."""
+    import torch
+    o, p = _pair(13, 11, N)
+    bc = _bcs(o)[bcname]
+    op = p.device_operator(bc, 0.5)
+    u = np.random.default_rng(N + 20).standard_normal((o.Np, o.K))
+    flat = torch.as_tensor(u.T.reshape(-1).copy(), device="cuda").float()
+    for alpha in (0.0, 5.0):
+        ref = osp.flat_op(o, bc_types=bc, alpha=alpha, tau_scale=0.5)(u.T.reshape(-1))
+        op.set_engine("tensor")
+        got_tc = op.apply(flat, alpha=alpha).double().cpu().numpy()
+        op.set_engine("cuda")
+        got_cc = op.apply(flat, alpha=alpha).double().cpu().numpy()
+        op.set_engine("tensor")
+        assert _rel(got_cc, ref) < APPLY_RTOL32, (N, bcname, alpha)
+        assert _rel(got_tc, ref) < APPLY_RTOL32, (N, bcname, alpha, _rel(got_tc, ref))
+
+
+def test_apply_fp32_tensor_cores_large_and_repeated():
+    """Persistent tensor-core kernel over many tiles (more tiles than CTAs),
+    run twice in a row: identical results, float32 accuracy."""
+    import torch
+    o, p = _pair(96, 80, 4)
+    bc = _bcs(o)["mixed"]
+    op = p.device_operator(bc, 0.5)
+    u = np.random.default_rng(5).standard_normal((o.Np, o.K))
+    flat = torch.as_tensor(u.T.reshape(-1).copy(), device="cuda").float()
+    y1 = op.apply(flat, alpha=5.0)
+    y2 = op.apply(flat, alpha=5.0)
+    torch.cuda.synchronize()
+    assert torch.equal(y1, y2)
+    ref = osp.flat_op(o, bc_types=bc, alpha=5.0, tau_scale=0.5)(u.T.reshape(-1))
+    assert _rel(y1.double().cpu().numpy(), ref) < APPLY_RTOL32
+
+
+def test_fp32_cg_tensor_and_cuda_engines_agree():
+    """float32 block-Jacobi PCG whose fused direction-update + apply runs on
+    the tensor cores converges like the CUDA-core one (same tolerance,
+    iteration counts within 10 %, solutions within float32 accuracy of the
+    float64 solve)."""
+    import torch
+    o, p = _pair(24, 20, 4)
+    bc = _bcs(o)["mixed"]
+    op = p.device_operator(bc, 0.5)
+    op.pc_build(alpha=5.0)
+    b = torch.as_tensor(np.random.default_rng(9).standard_normal(op.n), device="cuda")
+    x64 = torch.zeros_like(b)
+    st, it64, _, _ = op.cg(b, x64, tol=1e-10, maxiter=5000, pc=True, alpha=5.0)
+    assert st == "converged"
+    res = {}
+    for eng in ("tensor", "cuda"):
+        op.set_engine(eng)
+        x = torch.zeros_like(b, dtype=torch.float32)
+        st, its, _, _ = op.cg(b.float(), x, tol=1e-5, maxiter=5000, pc=True, alpha=5.0, precision="fp32")
+        assert st == "converged", eng
+        res[eng] = (its, x.double())
+    op.set_engine("tensor")
+    assert abs(res["tensor"][0] - res["cuda"][0]) <= max(3, 0.1 * res["cuda"][0])
+    for eng, (its, x) in res.items():
+        err = float((x - x64).norm() / x64.norm())
+        assert err < 1e-4, (eng, err)
+    # mixed precision (float32 iterations on the tensor cores, float64
+    # reliable updates) reaches the float64 tolerance
+    xm = torch.zeros_like(b)
+    st, its, rr, bb, upd = op.cg_mixed(b, xm, tol=1e-10, maxiter=20000, pc=True, alpha=5.0)
+    assert st == "converged"
+    assert float((xm - x64).norm() / x64.norm()) < 1e-8
