@@ -265,24 +265,60 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
     return;
   }
   const int tid = threadIdx.x;
-  const int k0 = blockIdx.x * BLOCK;
-  const int nk = min(BLOCK, a.K - k0);
-  const size_t off = (size_t)k0 * Np;
   const T al = INIT ? T(0) : T(a.ctl->alpha);
   double rr = 0.0, rz = 0.0, rp = 0.0;
-  for (int i = tid; i < nk * Np; i += BLOCK) {
-    T rn;
-    if (INIT) {
-      rn = a.r[off + i];
-      if (!a.keep_p) a.p_zero[off + i] = T(0);
-      else rp += (double)rn * (double)a.p_zero[off + i];
-    } else {
-      a.x[off + i] += al * a.p[off + i];
-      rn = a.r[off + i] - al * a.Ap[off + i];
-      a.r[off + i] = rn;
+  // persistent over element tiles: one partial per block, so the last
+  // block's reduction (the serial tail of the step) stays short
+  const int ntiles = (a.K + BLOCK - 1) / BLOCK;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const int k0 = tile * BLOCK;
+  const int nk = min(BLOCK, a.K - k0);
+  const size_t off = (size_t)k0 * Np;
+  if (!INIT && nk == BLOCK) {
+    // full tile: x += alpha p, r -= alpha Ap with the vectors marked
+    // non-aliasing and the loads of five tile rows issued together (the
+    // plain-pointer loop serialised every load behind the previous store)
+    T* __restrict__ x = a.x + off;
+    const T* __restrict__ p = a.p + off;
+    T* __restrict__ r = a.r + off;
+    const T* __restrict__ Ap = a.Ap + off;
+    constexpr int STEP = (Np % 5 == 0) ? 5 : ((Np % 3 == 0) ? 3 : 1);  // rows per batch, divides Np
+#pragma unroll
+    for (int c = 0; c < Np; c += STEP) {
+      T xv[STEP], pv[STEP], rv0[STEP], av[STEP];
+#pragma unroll
+      for (int u = 0; u < STEP; ++u) {
+        const int i = tid + (c + u) * BLOCK;
+        xv[u] = x[i];
+        pv[u] = __ldg(p + i);
+        rv0[u] = r[i];
+        av[u] = __ldg(Ap + i);
+      }
+#pragma unroll
+      for (int u = 0; u < STEP; ++u) {
+        const int i = tid + (c + u) * BLOCK;
+        x[i] = fma(al, pv[u], xv[u]);
+        const T rn = fma(-al, av[u], rv0[u]);
+        r[i] = rn;
+        rr += (double)rn * (double)rn;
+        if (PC) s_r[i] = rn;
+      }
     }
-    rr += (double)rn * (double)rn;
-    if (PC) s_r[i] = rn;
+  } else {
+    for (int i = tid; i < nk * Np; i += BLOCK) {
+      T rn;
+      if (INIT) {
+        rn = a.r[off + i];
+        if (!a.keep_p) a.p_zero[off + i] = T(0);
+        else rp += (double)rn * (double)a.p_zero[off + i];
+      } else {
+        a.x[off + i] += al * a.p[off + i];
+        rn = a.r[off + i] - al * a.Ap[off + i];
+        a.r[off + i] = rn;
+      }
+      rr += (double)rn * (double)rn;
+      if (PC) s_r[i] = rn;
+    }
   }
   if (PC) {
     // z = B^-1 r, one element per thread with the packed-symmetric indices
@@ -313,9 +349,10 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
     }
     __syncthreads();
     for (int i = tid; i < nk * Np; i += BLOCK) a.z[off + i] = s_r[i];
-  } else {
-    rz = rr;
+    __syncthreads();  // the next tile refills s_r
   }
+  }  // tiles
+  if (!PC) rz = rr;
   block_sum2<BLOCK>(rz, rr, s_red);
   if (INIT) {
     double d0 = 0.0;
@@ -357,6 +394,131 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(CgArgs<T> a) {
       cont = 0;
     }
     if (!INIT && !isfinite(c->beta)) {
+      c->status = 2;
+      cont = 0;
+    }
+    if (a.dev_status && *(volatile const unsigned int*)a.dev_status != 0u) {
+      c->status = 3;  // a kernel reported a device-side error: stop now
+      cont = 0;
+    }
+    if (cont == 0 && c->status == 0 && rs > c->atol2) c->status = 1;  // maxiter
+    c->cont = cont;
+    c->ticket = 0u;
+    if (a.has_cond) cudaGraphSetConditional(a.cond, (unsigned)cont);
+  }
+}
+
+// CG step with the element tiles staged by bulk copies (the regular
+// iteration, all vectors 16-byte aligned): thread 0 copies the x, p, r and
+// Ap tiles into shared memory at once, each thread updates its own element
+// (x += alpha p, r -= alpha Ap, z = B^-1 r with the packed-symmetric inverse
+// loaded once per entry), and the x, r, z tiles go back by bulk stores.
+// Same scalars, partials and loop control as k_cg_step.
+template <int N, typename T, bool PC, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_cg_step_bulk(CgArgs<T> a) {
+  constexpr int Np = Dim<N>::Np;
+  __shared__ __align__(128) T s_x[BLOCK * Np];
+  __shared__ __align__(128) T s_p[BLOCK * Np];   // p, then z
+  __shared__ __align__(128) T s_r[BLOCK * Np];
+  __shared__ __align__(128) T s_a[BLOCK * Np];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ double s_red[64];
+  __shared__ int s_ok;
+  if (a.ctl->cont == 0) {
+    if (a.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    return;
+  }
+  const int tid = threadIdx.x;
+  const int k0 = blockIdx.x * BLOCK, nk = min(BLOCK, a.K - k0);
+  const size_t off = (size_t)k0 * Np;
+  const uint32_t bytes = (uint32_t)(nk * Np * sizeof(T));
+  const bool bulk = (bytes % 16u) == 0u;  // the launcher checked the base alignment
+  const T al = T(a.ctl->alpha);
+  double rr = 0.0, rz = 0.0;
+  if (bulk) {
+    if (tid == 0) {
+      mbar_init(&s_bar, 1);
+      fence_mbar_init();
+      mbar_expect_tx(&s_bar, 4u * bytes);
+      bulk_load(s_x, a.x + off, bytes, &s_bar);
+      bulk_load(s_p, a.p + off, bytes, &s_bar);
+      bulk_load(s_r, a.r + off, bytes, &s_bar);
+      bulk_load(s_a, a.Ap + off, bytes, &s_bar);
+      s_ok = mbar_wait_bounded(&s_bar, 0, const_cast<unsigned int*>(a.dev_status)) ? 1 : 0;
+    }
+    __syncthreads();
+  } else {
+    for (int i = tid; i < nk * Np; i += BLOCK) {
+      s_x[i] = a.x[off + i];
+      s_p[i] = a.p[off + i];
+      s_r[i] = a.r[off + i];
+      s_a[i] = a.Ap[off + i];
+    }
+    if (tid == 0) s_ok = 1;
+    __syncthreads();
+  }
+  if (s_ok && tid < nk) {
+    T rv[Np];
+#pragma unroll
+    for (int i = 0; i < Np; ++i) {
+      const int j = tid * Np + i;
+      s_x[j] = fma(al, s_p[j], s_x[j]);
+      rv[i] = fma(-al, s_a[j], s_r[j]);
+      s_r[j] = rv[i];
+      rr += (double)rv[i] * (double)rv[i];
+    }
+    if (PC) {
+      T zv[Np];
+      sym_block_apply<Np, T>(a.binv + k0 + tid, (size_t)a.ldb, rv, zv);
+#pragma unroll
+      for (int i = 0; i < Np; ++i) {
+        s_p[tid * Np + i] = zv[i];  // own slots: p was read above
+        rz += (double)rv[i] * (double)zv[i];
+      }
+    } else {
+      rz = rr;
+    }
+  }
+  if (s_ok) {
+    if (bulk) {
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        bulk_store(a.x + off, s_x, bytes);
+        bulk_store(a.r + off, s_r, bytes);
+        if (PC) bulk_store(a.z + off, s_p, bytes);
+        bulk_commit();
+        bulk_wait_read_all();
+      }
+    } else {
+      __syncthreads();
+      for (int i = tid; i < nk * Np; i += BLOCK) {
+        a.x[off + i] = s_x[i];
+        a.r[off + i] = s_r[i];
+        if (PC) a.z[off + i] = s_p[i];
+      }
+    }
+  }
+  block_sum2<BLOCK>(rz, rr, s_red);
+  if (tid == 0) {
+    a.partA[blockIdx.x] = rz;
+    a.partB[blockIdx.x] = rr;
+  }
+  if (!is_last_block(&a.ctl->ticket)) return;
+  double g, r2, d1;
+  reduce_partials2<BLOCK>(a.partA, a.partB, gridDim.x, g, r2, s_red);
+  (void)d1;
+  if (tid == 0) {
+    CgCtl* c = a.ctl;
+    c->gamma_prev = c->gamma;
+    c->beta = g / c->gamma;
+    c->zcoef = 1.0;
+    c->iter += 1;
+    c->gamma = g;
+    c->rr = r2;
+    const double rs = c->use_pc ? r2 : g;
+    int cont = (rs > c->atol2) && (c->iter < c->maxiter) && (c->status == 0);
+    if (!isfinite(g) || !isfinite(r2) || !isfinite(c->beta)) {
       c->status = 2;
       cont = 0;
     }
@@ -862,16 +1024,52 @@ template cudaError_t launch_apply_nm<double>(int, const ApplyArgs<double>&, int,
 int apply_grid(int K) { return (K + 127) / 128; }
 int cg_grid(int K) { return (K + 127) / 128; }
 
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
+// Blocks of `kernel` that fill every SM once (occupancy API; cached per
+// kernel instantiation by the caller's static).
+template <typename Kern>
+static int full_wave(Kern kernel, int block) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return per_sm * sm_count();
+}
+
+template <int N, typename T, bool PC, bool INIT>
+static void launch_cg_one(const CgArgs<T>& a, cudaStream_t s) {
+  if (!INIT && a.bulk) {
+    // regular iteration with aligned vectors: tiles staged by bulk copies
+    constexpr int BB = sizeof(T) == 8 ? 64 : 128;  // four tiles within the 48 KB of static shared memory
+    k_cg_step_bulk<N, T, PC, BB><<<(a.K + BB - 1) / BB, BB, 0, s>>>(a);
+    return;
+  }
+  constexpr int B = 128;
+  static const int wave = full_wave(k_cg_step<N, T, PC, INIT, B>, B);
+  const int ntiles = (a.K + B - 1) / B;
+  // one resident wave at most: each block loops over tiles and publishes a
+  // single partial, so the serial last-block reduction stays short
+  k_cg_step<N, T, PC, INIT, B><<<ntiles < wave ? ntiles : wave, B, 0, s>>>(a);
+}
+
 template <int N, typename T>
 static cudaError_t launch_cg_n(bool pc, bool init, const CgArgs<T>& a, cudaStream_t s) {
-  constexpr int B = 128;
-  const int grid = (a.K + B - 1) / B;
   if (pc) {
-    if (init) k_cg_step<N, T, true, true, B><<<grid, B, 0, s>>>(a);
-    else k_cg_step<N, T, true, false, B><<<grid, B, 0, s>>>(a);
+    if (init) launch_cg_one<N, T, true, true>(a, s);
+    else launch_cg_one<N, T, true, false>(a, s);
   } else {
-    if (init) k_cg_step<N, T, false, true, B><<<grid, B, 0, s>>>(a);
-    else k_cg_step<N, T, false, false, B><<<grid, B, 0, s>>>(a);
+    if (init) launch_cg_one<N, T, false, true>(a, s);
+    else launch_cg_one<N, T, false, false>(a, s);
   }
   return cudaGetLastError();
 }

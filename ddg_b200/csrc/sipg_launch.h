@@ -53,6 +53,7 @@ struct CgArgs {
   int K;
   int has_cond;
   cudaGraphConditionalHandle cond;
+  int bulk;        // x, p, r, Ap, z 16-byte aligned: stage tiles by bulk copies
 };
 
 struct BlockArgs {

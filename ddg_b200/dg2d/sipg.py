@@ -44,7 +44,7 @@ class IterativeConfig:
     atol: float = 0.0
     maxiter: int = 1000
     precision: str = "fp64"      # "fp64" | "mixed" | "mixed-restart"
-    inner_tol: float = 0.1       # mixed: float32 residual reduction between float64 updates
+    inner_tol: float = 0.7       # mixed: float32 residual reduction between float64 updates
     max_refinements: int = 50    # mixed-restart: outer iteration cap
     restart: int = 30            # gmres
 

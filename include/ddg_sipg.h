@@ -102,13 +102,15 @@ int ddg_sipg_set_bc(ddg_sipg_op *op, const int32_t *bc_types);
 int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
                    const void *u, void *y, void *stream);
 
-/* Engine of the float32 operator apply (ddg_sipg_apply with DDG_FP32).
- * DDG_ENGINE_TENSOR_CORES (default for degrees 1..4): the element
- * contractions run on the tcgen05 tensor cores with 3xTF32 splitting
- * (float32-accurate); DDG_ENGINE_CUDA_CORES: plain float32 FMA on the CUDA
- * cores (the only engine for degree 5).  No reference counterpart (the
- * reference computes in float64 only); used by the float32 applies of the
- * mixed-precision solves. */
+/* Engine of the float32 operator applies.  DDG_ENGINE_TENSOR_CORES: the
+ * element contractions run on the tcgen05 tensor cores with 3xTF32
+ * splitting (float32-level accuracy, degrees 1..4); DDG_ENGINE_CUDA_CORES:
+ * plain float32 FMA on the CUDA cores (the only engine for degree 5).
+ * Defaults: stand-alone float32 applies (ddg_sipg_apply with DDG_FP32) use
+ * the tensor cores, float32 CG iterations (ddg_sipg_cg with DDG_FP32,
+ * ddg_sipg_cg_mixed) the CUDA cores, whose restarted mixed-precision
+ * iterations converge in fewer steps; calling this sets both.  No
+ * reference counterpart (the reference computes in float64 only). */
 #define DDG_ENGINE_CUDA_CORES   0
 #define DDG_ENGINE_TENSOR_CORES 1
 int ddg_sipg_set_engine(ddg_sipg_op *op, int engine);

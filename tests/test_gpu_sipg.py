@@ -405,3 +405,29 @@ def test_fp32_cg_tensor_and_cuda_engines_agree():
     st, its, rr, bb, upd = op.cg_mixed(b, xm, tol=1e-10, maxiter=20000, pc=True, alpha=5.0)
     assert st == "converged"
     assert float((xm - x64).norm() / x64.norm()) < 1e-8
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5])
+def test_apply_engines_match_oracle(N):
+    """Every apply engine against the oracle: float64 (1e-12), float32 CUDA
+    cores and tensor cores (float32 tolerance), with Helmholtz mass, mixed
+    BCs and a per-element diffusivity; odd element count (partial tiles)."""
+    import torch
+    o, p = _pair(9, 7, N)
+    bc = _bcs(o)["mixed"]
+    op = p.device_operator(bc, 0.5)
+    rng = np.random.default_rng(N + 40)
+    u = rng.standard_normal((o.Np, o.K))
+    flat = torch.as_tensor(u.T.reshape(-1).copy(), device="cuda")
+    for kappa in (None, np.exp(0.5 * rng.standard_normal(o.K))):
+        op.set_kappa(kappa)
+        ref = osp.flat_op(o, bc_types=bc, alpha=3.0, tau_scale=0.5, kappa=kappa)(u.T.reshape(-1))
+        got = op.apply(flat, alpha=3.0).cpu().numpy()
+        assert _rel(got, ref) < APPLY_RTOL64, (N, kappa is None)
+        for eng in ["cuda"] + (["tensor"] if N <= 4 else []):
+            op.set_engine(eng)
+            got = op.apply(flat.float(), alpha=3.0).double().cpu().numpy()
+            assert _rel(got, ref) < APPLY_RTOL32, (N, eng, kappa is None)
+    op.set_kappa(None)
+    if N <= 4:
+        op.set_engine("tensor")
