@@ -130,6 +130,9 @@ struct ddg_sipg_op {
   uint8_t* tc_img = nullptr;        // tensor-core B operands of this degree (device)
   int fp32_engine = DDG_ENGINE_TENSOR_CORES;   // stand-alone float32 applies
   int cg32_engine = DDG_ENGINE_CUDA_CORES;     // float32 CG iterations (fewer iterations in mixed solves)
+  double* dm_img = nullptr;         // FP64 tensor-core (DMMA) B operands of this degree (device)
+  double* dm_geo = nullptr;         // that kernel's element and face coefficients (device)
+  int fp64_engine = DDG_ENGINE_TENSOR_CORES;   // every float64 apply (stand-alone, CG, residuals)
 
 };
 
@@ -218,6 +221,10 @@ ApplyArgs<T> apply_args(ddg_sipg_op* op) {
   a.ldg = op->ldg;
   a.tau = op->tau;
   a.kappa = op->kappa_on ? ((sizeof(T) == 8) ? (const T*)op->kappa64 : (const T*)op->kappa32) : nullptr;
+  if (sizeof(T) == 8 && op->fp64_engine == DDG_ENGINE_TENSOR_CORES) {
+    a.dm_img = op->dm_img;
+    a.dm_geo = op->dm_geo;
+  }
   return a;
 }
 
@@ -326,6 +333,8 @@ void free_op(ddg_sipg_op* op) {
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
   }
   if (op->tc_img) cudaFree(op->tc_img);
+  if (op->dm_img) cudaFree(op->dm_img);
+  if (op->dm_geo) cudaFree(op->dm_geo);
 
   void* ptrs[] = {op->kappa64, op->kappa32, op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
                   op->ticket, op->dotbuf, op->blocks, op->binv64, op->binv32};
@@ -495,6 +504,18 @@ extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
     if (e == cudaSuccess) e = tc_prepare(N);
   }
   if (!tc_supported(N)) op->fp32_engine = DDG_ENGINE_CUDA_CORES;
+  if (e == cudaSuccess && dm_supported(N)) {
+    std::vector<double> img((size_t)dm_image_doubles(N), 0.0);
+    dm_build_image(N, d->Dr, d->Ds, d->M, d->m1d, img.data());
+    e = cudaMalloc((void**)&op->dm_img, img.size() * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(op->dm_img, img.data(), img.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = dm_prepare(N);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&op->dm_geo, (size_t)dm_geo_fields() * op->ldg * sizeof(double));
+    if (e == cudaSuccess) e = dm_build_geo(op->geo64, op->nbr, op->dm_geo, op->K, op->ldg, op->tau, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  if (!op->dm_img || !op->dm_geo) op->fp64_engine = DDG_ENGINE_CUDA_CORES;
   if (e != cudaSuccess) {
     free_op(op);
     return fail(e == cudaErrorMemoryAllocation ? DDG_ERR_NOMEM : DDG_ERR_CUDA,
@@ -518,6 +539,10 @@ extern "C" int ddg_sipg_set_bc(ddg_sipg_op* op, const int32_t* bc) {
   int rc = build_nbr(op, bc);
   if (rc != DDG_OK) return rc;
   CK(cudaMemcpy(op->nbr, op->nbr_host.data(), op->nbr_host.size() * 4, cudaMemcpyHostToDevice));
+  if (op->dm_geo) {
+    CK(dm_build_geo(op->geo64, op->nbr, op->dm_geo, op->K, op->ldg, op->tau, nullptr));
+    CK(cudaDeviceSynchronize());
+  }
   op->pc_ready = false;
   if (op->hio) op->hio->need.clear();
   return DDG_OK;
@@ -668,13 +693,14 @@ extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* 
 extern "C" int ddg_sipg_set_engine(ddg_sipg_op* op, int engine) {
   if (!op) return fail(DDG_ERR_INVALID, "ddg_sipg_set_engine: null handle");
   if (engine == DDG_ENGINE_CUDA_CORES) {
-    op->fp32_engine = op->cg32_engine = engine;
+    op->fp32_engine = op->cg32_engine = op->fp64_engine = engine;
     return DDG_OK;
   }
   if (engine == DDG_ENGINE_TENSOR_CORES) {
-    if (!op->tc_img)
-      return fail(DDG_ERR_UNSUPPORTED, "tensor-core float32 apply is built for degrees 1..4 only");
-    op->fp32_engine = op->cg32_engine = engine;
+    if (!op->tc_img && !op->dm_img)
+      return fail(DDG_ERR_UNSUPPORTED, "no tensor-core apply is built for this degree");
+    if (op->tc_img) op->fp32_engine = op->cg32_engine = engine;
+    if (op->dm_img) op->fp64_engine = engine;
     return DDG_OK;
   }
   return fail(DDG_ERR_INVALID, "engine must be DDG_ENGINE_CUDA_CORES or DDG_ENGINE_TENSOR_CORES");
@@ -775,7 +801,7 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
   Work& w = op->w[prec];
   cudaStream_t s = (cudaStream_t)stream;
   GraphKey key{prec, cfg->pc, cfg->alpha, cfg->shift};
-  key.engine = (prec == DDG_FP32 && op->tc_img) ? op->cg32_engine : DDG_ENGINE_CUDA_CORES;
+  key.engine = prec == DDG_FP32 ? (op->tc_img ? op->cg32_engine : DDG_ENGINE_CUDA_CORES) : op->fp64_engine;
   CgGraph* gr = nullptr;
   rc = get_graph(op, key, &gr);
   if (rc != DDG_OK) return rc;
@@ -1342,6 +1368,7 @@ extern "C" int ddg_sipg_cg_mg(ddg_sipg_op* op, const ddg_cg_config* cfg, ddg_mg*
   Work& w = op->w[DDG_FP64];
   cudaStream_t s = (cudaStream_t)stream;
   GraphKey key{DDG_FP64, 99, cfg->alpha, cfg->shift};
+  key.engine = op->fp64_engine;
   CgGraph* gr = nullptr;
   rc = get_mg_graph(op, mg, key, &gr);
   if (rc != DDG_OK) return rc;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -973,6 +974,9 @@ template <typename T> constexpr int apply_block() { return sizeof(T) == 8 ? 128 
 
 template <int N, typename T>
 static cudaError_t launch_apply_n(int mode, const ApplyArgs<T>& a, cudaStream_t s) {
+  if constexpr (sizeof(T) == 8) {
+    if (dm_handles(mode, a)) return launch_apply_dm(N, mode, a, s);
+  }
   constexpr int B = apply_block<T>();
   const int grid = (a.K + B - 1) / B;
   switch (mode) {
@@ -1181,3 +1185,4 @@ cudaError_t launch_dot(int64_t n, int prec, const void* x, const void* y, double
 
 #include "sipg_batch_kernels.cuh"
 #include "sipg_tc.cuh"
+#include "sipg_dm.cuh"

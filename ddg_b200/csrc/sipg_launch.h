@@ -32,6 +32,8 @@ struct ApplyArgs {
   int ldb;
   double omega;             // SMOOTH: damping
   const T* kappa;           // per-element diffusivity (null: 1)
+  const double* dm_img;     // float64: FP64 tensor-core operand image (null: CUDA cores)
+  const double* dm_geo;     // float64: that kernel's element and face coefficients ([D_COUNT][ldg])
 };
 
 template <typename T>
@@ -126,6 +128,21 @@ int tc_build_image(int N, const double* Dr, const double* Ds, const double* M, u
 // modes AM_APPLY and AM_PFUSE; tc_prepare sets the kernels' attributes
 cudaError_t tc_prepare(int N);
 cudaError_t launch_apply_tc(int N, int mode, const ApplyArgs<float>& a, const uint8_t* img, cudaStream_t s);
+// float64 apply on the FP64 tensor cores (mma.sync f64, degrees 1..5):
+// modes AM_APPLY, AM_PFUSE, AM_RESID without kappa; launch_apply<double>
+// dispatches to it whenever ApplyArgs::dm_img is set.  dm_prepare sets the
+// kernels' shared-memory attribute and occupancy (once per degree).
+bool dm_supported(int N);
+int dm_image_doubles(int N);
+int dm_build_image(int N, const double* Dr, const double* Ds, const double* M, const double* m1d, double* out);
+cudaError_t dm_prepare(int N);
+bool dm_handles(int mode, const ApplyArgs<double>& a);
+int dm_geo_fields();
+// element and face coefficients of the FP64 tensor-core kernel from the
+// geometry and the neighbour words (again after every boundary-tag change)
+cudaError_t dm_build_geo(const double* geo, const uint32_t* nbr, double* dg, int K, int ldg, double tau,
+                         cudaStream_t s);
+cudaError_t launch_apply_dm(int N, int mode, const ApplyArgs<double>& a, cudaStream_t s);
 // node-major (Np, K) fields, elements [k_begin, k_end) only (in0 -> out0)
 template <typename T>
 cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s);

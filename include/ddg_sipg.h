@@ -102,15 +102,19 @@ int ddg_sipg_set_bc(ddg_sipg_op *op, const int32_t *bc_types);
 int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
                    const void *u, void *y, void *stream);
 
-/* Engine of the float32 operator applies.  DDG_ENGINE_TENSOR_CORES: the
+/* Engine of the operator applies.  DDG_ENGINE_TENSOR_CORES: float32
  * element contractions run on the tcgen05 tensor cores with 3xTF32
- * splitting (float32-level accuracy, degrees 1..4); DDG_ENGINE_CUDA_CORES:
- * plain float32 FMA on the CUDA cores (the only engine for degree 5).
- * Defaults: stand-alone float32 applies (ddg_sipg_apply with DDG_FP32) use
- * the tensor cores, float32 CG iterations (ddg_sipg_cg with DDG_FP32,
+ * splitting (float32-level accuracy, degrees 1..4), float64 ones on the
+ * FP64 tensor cores (mma.sync f64, float64 arithmetic, degrees 1..5; not
+ * with a per-element diffusivity); DDG_ENGINE_CUDA_CORES: plain FMA on the
+ * CUDA cores.  Defaults: every float64 apply (ddg_sipg_apply with DDG_FP64,
+ * float64 CG and residuals) and stand-alone float32 applies use the tensor
+ * cores; float32 CG iterations (ddg_sipg_cg with DDG_FP32,
  * ddg_sipg_cg_mixed) the CUDA cores, whose restarted mixed-precision
- * iterations converge in fewer steps; calling this sets both.  No
- * reference counterpart (the reference computes in float64 only). */
+ * iterations converge in fewer steps.  Calling this sets all three where
+ * the degree has the engine (DDG_ERR_UNSUPPORTED if it has none).  No
+ * reference counterpart (the reference's operator is jax.grad of its
+ * bilinear form, sipg.py:304-337). */
 #define DDG_ENGINE_CUDA_CORES   0
 #define DDG_ENGINE_TENSOR_CORES 1
 int ddg_sipg_set_engine(ddg_sipg_op *op, int engine);
