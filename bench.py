@@ -241,10 +241,11 @@ def run_ours(args, rank, world, local_rank):
         "apply_fp32": {"gdofs": n / a32 / 1e9, "us": a32 * 1e6},
         "roofline": {"bound": "hbm", "achieved": B64 / a64 / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": B64 / a64 / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "k_apply<4,double,APPLY>", "algorithmic_bytes": B64},
+                     "kernel": "k_apply_dm<4,APPLY> (FP64 tensor cores, mma.sync m16n8k8 f64)",
+                     "algorithmic_bytes": B64},
         "roofline_fp32": {"bound": "hbm", "achieved": B32 / a32 / 1e9, "peak": hbm, "unit": "GB/s",
                           "frac": B32 / a32 / 1e9 / hbm,
-                          "kernel": "k_trace_tc<4,APPLY> + k_flux_tc<4,APPLY> (tcgen05, TF32 split 3 ways)",
+                          "kernel": "k_apply_tc<4,APPLY> (tcgen05 kind::tf32, 3xTF32 split)",
                           "algorithmic_bytes": B32},
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,

@@ -436,3 +436,53 @@ def test_apply_engines_match_oracle(N):
     op.set_kappa(None)
     if N <= 4:
         op.set_engine("tensor")
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5])
+def test_fp64_engines_match_oracle_and_each_other(N):
+    """float64 apply on the FP64 tensor cores (the default engine) and on the
+    CUDA cores against the oracle (1e-12) for Poisson and Helmholtz under
+    every BC set, switched with set_bc (which rebuilds the tensor-core
+    kernel's face table), on an odd element count (partial row blocks)."""
+    import torch
+    o, p = _pair(9, 7, N)
+    bcs = _bcs(o)
+    op = p.device_operator(bcs["mixed"], 0.5)
+    rng = np.random.default_rng(N + 70)
+    u = rng.standard_normal((o.Np, o.K))
+    flat = torch.as_tensor(u.T.reshape(-1).copy(), device="cuda")
+    for name in ("mixed", "dirichlet", "neumann", "interior_tagged_boundary", "mixed"):
+        op.set_bc(bcs[name])
+        for alpha in (0.0, 3.0):
+            ref = osp.flat_op(o, bc_types=bcs[name], alpha=alpha, tau_scale=0.5)(u.T.reshape(-1))
+            got = {}
+            for eng in ("tensor", "cuda"):
+                op.set_engine(eng)
+                got[eng] = op.apply(flat, alpha=alpha).cpu().numpy()
+                assert _rel(got[eng], ref) < APPLY_RTOL64, (N, name, alpha, eng)
+            assert _rel(got["tensor"], got["cuda"]) < 1e-13, (N, name, alpha)
+    op.set_engine("tensor")
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_fp64_cg_engines_agree(N):
+    """float64 block-Jacobi PCG through the FP64 tensor-core kernel's CG
+    modes (direction update fused with the apply, residual with norms)
+    against the CUDA-core engine: iteration counts within 2, solutions
+    within 1e-9 relative."""
+    import torch
+    o, p = _pair(12, 10, N)
+    bc = _bcs(o)["mixed"]
+    op = p.device_operator(bc, 0.5)
+    op.pc_build(alpha=2.0)
+    b = torch.as_tensor(np.random.default_rng(5).standard_normal(op.n), device="cuda")
+    res = {}
+    for eng in ("tensor", "cuda"):
+        op.set_engine(eng)
+        x = torch.zeros_like(b)
+        st = op.cg(b, x, tol=1e-12, maxiter=5000, pc=True, alpha=2.0)
+        assert st[0] == "converged", (eng, st)
+        res[eng] = (st[1], x.cpu().numpy())
+    op.set_engine("tensor")
+    assert abs(res["tensor"][0] - res["cuda"][0]) <= 2
+    assert np.linalg.norm(res["tensor"][1] - res["cuda"][1]) / np.linalg.norm(res["cuda"][1]) < 1e-9
