@@ -75,22 +75,38 @@ struct CgGraph {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+#ifndef DDG_HOST_CHUNKS
+#define DDG_HOST_CHUNKS 8   // element chunks of the host-buffer apply pipeline
+#endif
+
 // State of the host-buffer apply (ddg_sipg_apply_host), created on first use:
 // node-major device copies of u and y, pinned staging for pageable host
 // arrays, one stream per direction plus one for the kernels, and per-chunk
-// events.  need[c] is the last element chunk whose values chunk c's
-// elements read through a face (neighbours), so chunk c's kernel waits only
-// for the host->device copies up to need[c].
+// events.  Each chunk's elements are applied in two pieces: the leading
+// run whose neighbours all lie in chunks <= c (ready as soon as chunk c has
+// arrived) and the rest; need[i] is the last chunk piece i reads through a
+// face, so its kernel waits only for the host->device copies up to need[i].  With pinned host arrays the
+// whole chunked pipeline (about 8 API calls per chunk) is captured once per
+// (u, y, alpha) into a CUDA graph and replayed with one launch.
 struct HostIO {
-  double* d_u = nullptr;
-  double* d_y = nullptr;
+  double* d_u = nullptr;   // node-major input, as copied from the host
+  double* d_y = nullptr;   // node-major output, copied to the host
+  double* e_u = nullptr;   // element-major input (transposed on the device)
+  double* e_y = nullptr;   // element-major output of the apply
   double* h_u = nullptr;   // pinned staging (pageable input)
   double* h_y = nullptr;   // pinned staging (pageable output)
   cudaStream_t s_in = nullptr, s_cmp = nullptr, s_out = nullptr;
   cudaEvent_t e_start = nullptr;
   std::vector<cudaEvent_t> e_in, e_cmp, e_out;
-  std::vector<int> need;
+  std::vector<int> need;                 // per piece (2 per chunk), running maximum
+  std::vector<int> p_lo, p_hi;           // piece element ranges
   int nch = 0, chunk = 0;
+  cudaStream_t s_org = nullptr;       // capture origin of the pipeline graph
+  cudaGraphExec_t gexec = nullptr;    // the captured pipeline for (g_u, g_y, g_alpha)
+  const double* g_u = nullptr;
+  double* g_y = nullptr;
+  double g_alpha = 0.0;
+  bool g_ok = false;
 };
 
 }  // namespace
@@ -349,12 +365,15 @@ void free_op(ddg_sipg_op* op) {
   if (HostIO* h = op->hio) {
     if (h->d_u) cudaFree(h->d_u);
     if (h->d_y) cudaFree(h->d_y);
+    if (h->e_u) cudaFree(h->e_u);
+    if (h->e_y) cudaFree(h->e_y);
     if (h->h_u) cudaFreeHost(h->h_u);
     if (h->h_y) cudaFreeHost(h->h_y);
     for (auto* v : {&h->e_in, &h->e_cmp, &h->e_out})
       for (cudaEvent_t ev : *v) cudaEventDestroy(ev);
     if (h->e_start) cudaEventDestroy(h->e_start);
-    for (cudaStream_t st : {h->s_in, h->s_cmp, h->s_out})
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (cudaStream_t st : {h->s_in, h->s_cmp, h->s_out, h->s_org})
       if (st) cudaStreamDestroy(st);
     delete h;
   }
@@ -587,39 +606,55 @@ int hio_prepare(ddg_sipg_op* op) {
   if (!op->hio) {
     HostIO* h = new HostIO();
     op->hio = h;  // released by free_op even when set-up stops halfway
-    h->nch = std::max(1, std::min(16, K / 4096));
-    h->chunk = (K + h->nch - 1) / h->nch;
+    // pitched copies of 15 rows lose bandwidth as chunks shrink, and copies in
+    // both directions overlap best with few large chunks (measured on B200:
+    // 4-8 chunks of 1.9-3.9 MB); the chunk pipeline needs at least a few
+    h->nch = std::max(1, std::min(DDG_HOST_CHUNKS, K / 4096));
+    h->chunk = ((K + h->nch - 1) / h->nch + 63) / 64 * 64;  // element ranges start on 64-element tiles
     h->nch = (K + h->chunk - 1) / h->chunk;
     const size_t bytes = (size_t)K * op->Np * sizeof(double);
     CK(cudaMalloc((void**)&h->d_u, bytes));
     CK(cudaMalloc((void**)&h->d_y, bytes));
+    CK(cudaMalloc((void**)&h->e_u, bytes));
+    CK(cudaMalloc((void**)&h->e_y, bytes));
     CK(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->s_cmp, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->s_org, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->e_start, cudaEventDisableTiming));
-    for (auto* v : {&h->e_in, &h->e_cmp, &h->e_out}) {
-      v->assign(h->nch, nullptr);
+    h->e_in.assign(h->nch, nullptr);
+    h->e_cmp.assign(2 * h->nch, nullptr);
+    h->e_out.assign(2 * h->nch, nullptr);
+    for (auto* v : {&h->e_in, &h->e_cmp, &h->e_out})
       for (cudaEvent_t& ev : *v) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    }
   }
   HostIO* h = op->hio;
   if (h->need.empty()) {
-    // chunk c reads the values of every element that shares a face with one
-    // of its elements (neighbour words with the own-interior or
-    // neighbour-side bit set); kernels launch in chunk order, so keep the
-    // running maximum
-    std::vector<int> need(h->nch);
-    for (int c = 0; c < h->nch; ++c) need[c] = c;
+    // mx[k]: the last chunk element k reads (its own, or a neighbour's through
+    // a face whose own-interior or neighbour-side bit is set)
+    std::vector<int> mx(K);
+    for (int k = 0; k < K; ++k) mx[k] = k / h->chunk;
     for (int f = 0; f < 3; ++f)
       for (int k = 0; k < K; ++k) {
         const uint32_t w = op->nbr_host[(size_t)f * K + k];
-        if (w & (32u | 64u)) {
-          const int c = k / h->chunk, cp = (int)(w >> 7) / h->chunk;
-          if (cp > need[c]) need[c] = cp;
-        }
+        if (w & (32u | 64u)) mx[k] = std::max(mx[k], (int)(w >> 7) / h->chunk);
       }
-    for (int c = 1; c < h->nch; ++c) need[c] = std::max(need[c], need[c - 1]);
+    std::vector<int> need(2 * h->nch), lo(2 * h->nch), hi(2 * h->nch);
+    for (int c = 0; c < h->nch; ++c) {
+      const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
+      int p = c0;
+      while (p < c1 && mx[p] <= c) ++p;
+      if (p < c1) p = c0 + (p - c0) / 16 * 16;  // ranges of the tensor-core kernel start on 16-element blocks
+      int tail = c;
+      for (int k = p; k < c1; ++k) tail = std::max(tail, mx[k]);
+      lo[2 * c] = c0, hi[2 * c] = p, need[2 * c] = c;
+      lo[2 * c + 1] = p, hi[2 * c + 1] = c1, need[2 * c + 1] = tail;
+    }
+    for (size_t i = 1; i < need.size(); ++i) need[i] = std::max(need[i], need[i - 1]);
     h->need.swap(need);
+    h->p_lo.swap(lo);
+    h->p_hi.swap(hi);
+    h->g_ok = false;  // the captured pipeline followed the old dependencies
   }
   return DDG_OK;
 }
@@ -636,39 +671,47 @@ bool host_pinned(const void* p) {
 
 }  // namespace
 
-extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* u, double* y, void* stream) {
-  if (!op || !u || !y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: null argument");
-  if ((const void*)u == (const void*)y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: u and y must not alias");
-  DevGuard guard(op->dev);
-  int rc = hio_prepare(op);
-  if (rc != DDG_OK) return rc;
+namespace {
+
+// Issue the chunked pipeline for pinned (or staged) host arrays src -> dst
+// after the work already queued on `us`, and join it back into `us`.  Per
+// element chunk: a pitched copy engine transfer of the chunk's Np row
+// segments (few large chunks: copies in both directions then overlap), a
+// transpose to the element-major layout in device memory, the element-major
+// apply of every chunk whose neighbours have all arrived (the tensor-core
+// kernel for float64 where built), the transpose back and the pitched copy
+// to the host.  With stage_u, chunk c of the pageable input u is first
+// copied into the pinned staging buffer (host memcpy; not capturable).
+int hio_issue(ddg_sipg_op* op, double alpha, const double* u, const double* src, double* dst, bool stage_u,
+              cudaStream_t us) {
   HostIO* h = op->hio;
   const int K = op->K, Np = op->Np;
-  const size_t pitch = (size_t)K * sizeof(double), bytes = pitch * Np;
-  const bool u_pin = host_pinned(u), y_pin = host_pinned(y);
-  if (!u_pin && !h->h_u) CK(cudaMallocHost((void**)&h->h_u, bytes));
-  if (!y_pin && !h->h_y) CK(cudaMallocHost((void**)&h->h_y, bytes));
-  cudaStream_t us = (cudaStream_t)stream;
+  const size_t pitch = (size_t)K * sizeof(double);
   CK(cudaEventRecord(h->e_start, us));
   for (cudaStream_t st : {h->s_in, h->s_cmp, h->s_out}) CK(cudaStreamWaitEvent(st, h->e_start, 0));
   ApplyArgs<double> a = apply_args<double>(op);
-  a.in0 = h->d_u;
-  a.out0 = h->d_y;
+  a.in0 = h->e_u;
+  a.out0 = h->e_y;
   a.alpha = alpha;
-  const double* src = u_pin ? u : h->h_u;
-  double* dst = y_pin ? y : h->h_y;
+  a.use_tma = aligned16(h->e_u) && aligned16(h->e_y);
   int next = 0;
   for (int c = 0; c < h->nch; ++c) {
     const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
     const size_t w = (size_t)(c1 - c0) * sizeof(double);
-    if (!u_pin)  // stage this chunk while the previous one is in flight
+    if (stage_u)  // stage this chunk while the previous one is in flight
       for (int i = 0; i < Np; ++i) std::memcpy(h->h_u + (size_t)i * K + c0, u + (size_t)i * K + c0, w);
     CK(cudaMemcpy2DAsync(h->d_u + c0, pitch, src + c0, pitch, w, Np, cudaMemcpyHostToDevice, h->s_in));
     CK(cudaEventRecord(h->e_in[c], h->s_in));
-    for (; next < h->nch && h->need[next] <= c; ++next) {
-      const int j0 = next * h->chunk, j1 = std::min(K, j0 + h->chunk);
-      CK(cudaStreamWaitEvent(h->s_cmp, h->e_in[c], 0));
-      const cudaError_t e = launch_apply_nm<double>(op->N, a, j0, j1, h->s_cmp);
+    CK(cudaStreamWaitEvent(h->s_cmp, h->e_in[c], 0));
+    cudaError_t e = launch_nm_to_em(h->d_u, h->e_u, K, Np, c0, c1, h->s_cmp);
+    if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("transpose launch: ") + cudaGetErrorString(e));
+    for (; next < 2 * h->nch && h->need[next] <= c; ++next) {
+      const int j0 = h->p_lo[next], j1 = h->p_hi[next];
+      if (j1 <= j0) continue;
+      a.k_lo = j0;
+      a.k_hi = j1;
+      e = launch_apply<double>(op->N, AM_APPLY, a, h->s_cmp);
+      if (e == cudaSuccess) e = launch_em_to_nm(h->e_y, h->d_y, K, Np, j0, j1, h->s_cmp);
       if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("apply launch: ") + cudaGetErrorString(e));
       CK(cudaEventRecord(h->e_cmp[next], h->s_cmp));
       CK(cudaStreamWaitEvent(h->s_out, h->e_cmp[next], 0));
@@ -677,15 +720,82 @@ extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* 
       CK(cudaEventRecord(h->e_out[next], h->s_out));
     }
   }
+  // join: every stream's last piece covers everything issued on it
+  int last = 2 * h->nch - 1;
+  while (last > 0 && h->p_hi[last] <= h->p_lo[last]) --last;
+  CK(cudaStreamWaitEvent(us, h->e_in[h->nch - 1], 0));
+  CK(cudaStreamWaitEvent(us, h->e_cmp[last], 0));
+  CK(cudaStreamWaitEvent(us, h->e_out[last], 0));
+  return DDG_OK;
+}
+
+// Capture the pinned-array pipeline for (u, y, alpha) into h->gexec.
+int hio_capture(ddg_sipg_op* op, double alpha, const double* u, double* y) {
+  HostIO* h = op->hio;
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+  h->g_ok = false;
+  CK(cudaStreamBeginCapture(h->s_org, cudaStreamCaptureModeThreadLocal));
+  const int rc = hio_issue(op, alpha, u, u, y, false, h->s_org);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(h->s_org, &g);
+  if (rc != DDG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e2 != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("host-buffer graph capture: ") + cudaGetErrorString(e2));
+  const cudaError_t e3 = cudaGraphInstantiate(&h->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) {
+    h->gexec = nullptr;
+    return fail(DDG_ERR_CUDA, std::string("host-buffer graph instantiate: ") + cudaGetErrorString(e3));
+  }
+  h->g_u = u;
+  h->g_y = y;
+  h->g_alpha = alpha;
+  h->g_ok = true;
+  return DDG_OK;
+}
+
+}  // namespace
+
+extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* u, double* y, void* stream) {
+  if (!op || !u || !y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: null argument");
+  if ((const void*)u == (const void*)y) return fail(DDG_ERR_INVALID, "ddg_sipg_apply_host: u and y must not alias");
+  DevGuard guard(op->dev);
+  int rc = hio_prepare(op);
+  if (rc != DDG_OK) return rc;
+  HostIO* h = op->hio;
+  const int K = op->K, Np = op->Np;
+  const size_t bytes = (size_t)K * Np * sizeof(double);
+  const bool u_pin = host_pinned(u), y_pin = host_pinned(y);
+  cudaStream_t us = (cudaStream_t)stream;
+  if (u_pin && y_pin) {
+    // one graph launch replays the whole pipeline for these arrays
+    if (!(h->g_ok && h->g_u == u && h->g_y == y && h->g_alpha == alpha)) {
+      rc = hio_capture(op, alpha, u, y);
+      if (rc != DDG_OK) return rc;
+    }
+    CK(cudaGraphLaunch(h->gexec, us));
+    CK(cudaStreamSynchronize(us));
+    return DDG_OK;
+  }
+  if (!u_pin && !h->h_u) CK(cudaMallocHost((void**)&h->h_u, bytes));
+  if (!y_pin && !h->h_y) CK(cudaMallocHost((void**)&h->h_y, bytes));
+  const double* src = u_pin ? u : h->h_u;
+  double* dst = y_pin ? y : h->h_y;
+  rc = hio_issue(op, alpha, u, src, dst, !u_pin, us);
+  if (rc != DDG_OK) return rc;
   if (!y_pin) {
-    for (int j = 0; j < h->nch; ++j) {
-      const int j0 = j * h->chunk, j1 = std::min(K, j0 + h->chunk);
+    for (int j = 0; j < 2 * h->nch; ++j) {
+      const int j0 = h->p_lo[j], j1 = h->p_hi[j];
+      if (j1 <= j0) continue;
       CK(cudaEventSynchronize(h->e_out[j]));
       for (int i = 0; i < Np; ++i)
         std::memcpy(y + (size_t)i * K + j0, h->h_y + (size_t)i * K + j0, (size_t)(j1 - j0) * sizeof(double));
     }
   } else {
-    CK(cudaStreamSynchronize(h->s_out));
+    CK(cudaStreamSynchronize(us));
   }
   return DDG_OK;
 }
@@ -1426,6 +1536,7 @@ void drop_graphs(ddg_sipg_op* op) {
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
   }
   op->mg_graphs.clear();
+  if (op->hio) op->hio->g_ok = false;
 }
 }  // namespace
 

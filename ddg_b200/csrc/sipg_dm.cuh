@@ -190,10 +190,13 @@ __global__ void __launch_bounds__(BLOCK, (N <= 4 ? 2 : 1)) k_apply_dm(ApplyArgs<
   uint32_t phase = 0;
   bool dead = (s_ok == 0);
   bool pending = false;  // a bulk store of this warp may still read its tiles
-  const int nrb = (K + RB - 1) / RB;
-  for (int rb = blockIdx.x * WARPS + warp; rb < nrb && !dead; rb += gridDim.x * WARPS) {
+  // AM_APPLY may cover the element range [k_lo, k_hi) only (k_lo a multiple of RB)
+  const int k_hi = (MODE == AM_APPLY && a.k_hi > 0) ? a.k_hi : K;
+  const int rb_lo = (MODE == AM_APPLY) ? a.k_lo / RB : 0;
+  const int nrb = (k_hi + RB - 1) / RB;
+  for (int rb = rb_lo + blockIdx.x * WARPS + warp; rb < nrb && !dead; rb += gridDim.x * WARPS) {
     const int k0 = rb * RB;
-    const int nw = min(RB, K - k0);
+    const int nw = min(RB, k_hi - k0);
     const size_t off = (size_t)k0 * Np;
     const uint32_t bytes = (uint32_t)(nw * Np * 8);
     const bool tma = a.use_tma && (bytes % 16u == 0u);
@@ -567,7 +570,10 @@ template <int N, int MODE>
 cudaError_t launch_one(const ApplyArgs<double>& a, cudaStream_t s) {
   const int nb = occ().blocks[N][MODE];
   if (nb <= 0) return cudaErrorInitializationError;  // dm_prepare not called for this degree
-  const int nrb = (a.K + RB - 1) / RB;
+  const bool ranged = MODE == AM_APPLY && a.k_hi > 0;
+  if (ranged && (a.k_lo % RB != 0 || a.k_hi > a.K || a.k_lo < 0)) return cudaErrorInvalidValue;
+  const int nrb = ranged ? (a.k_hi + RB - 1) / RB - a.k_lo / RB : (a.K + RB - 1) / RB;
+  if (nrb <= 0) return cudaSuccess;
   const int grid = std::max(1, std::min((nrb + WARPS - 1) / WARPS, nb * sm_count()));
   k_apply_dm<N, MODE><<<grid, BLOCK, shape_of(N).smem, s>>>(a);
   return cudaGetLastError();

@@ -56,8 +56,9 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
 
   if (MODE == AM_PFUSE && a.ctl->cont == 0) return;  // uniform across the grid
   const int tid = threadIdx.x;
-  const int k0 = blockIdx.x * BLOCK;
-  const int nk = min(BLOCK, a.K - k0);
+  const int k_hi = (MODE == AM_APPLY && a.k_hi > 0) ? a.k_hi : a.K;
+  const int k0 = (MODE == AM_APPLY ? a.k_lo : 0) + blockIdx.x * BLOCK;
+  const int nk = min(BLOCK, k_hi - k0);
   const size_t off = (size_t)k0 * Np;
   const uint32_t bytes = (uint32_t)(nk * Np * sizeof(T));
   const bool tma = a.use_tma && (bytes % 16u == 0u);
@@ -978,7 +979,9 @@ static cudaError_t launch_apply_n(int mode, const ApplyArgs<T>& a, cudaStream_t 
     if (dm_handles(mode, a)) return launch_apply_dm(N, mode, a, s);
   }
   constexpr int B = apply_block<T>();
-  const int grid = (a.K + B - 1) / B;
+  const int span = (mode == AM_APPLY && a.k_hi > 0) ? a.k_hi - a.k_lo : a.K;
+  if (span <= 0) return cudaSuccess;
+  const int grid = (span + B - 1) / B;
   switch (mode) {
     case AM_APPLY: k_apply<N, T, AM_APPLY, B><<<grid, B, 0, s>>>(a); break;
     case AM_PFUSE: k_apply<N, T, AM_PFUSE, B><<<grid, B, 0, s>>>(a); break;
@@ -1024,6 +1027,53 @@ cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end
   return cudaErrorInvalidValue;
 }
 template cudaError_t launch_apply_nm<double>(int, const ApplyArgs<double>&, int, int, cudaStream_t);
+
+// Node-major (rows, ld) <-> element-major (ld, rows) transposes of elements
+// [k0, k1) for the host-buffer apply (its host arrays are the reference's
+// (Np, K) layout).  Tiles of 64 elements: the node-major side is read or
+// written one row segment (64 consecutive doubles) at a time, the
+// element-major side as one contiguous 64 x rows block; both coalesced.
+template <bool TO_EM>
+__global__ void __launch_bounds__(256) k_transpose_nm(const double* __restrict__ src, double* __restrict__ dst,
+                                                      int ld, int rows, int k0, int k1) {
+  extern __shared__ double s_t[];  // [rows][65]
+  const int kb = k0 + blockIdx.x * 64, nk = min(64, k1 - kb);
+  if (nk <= 0) return;
+  if (TO_EM) {
+    for (int i = threadIdx.x; i < rows * 64; i += 256) {
+      const int r = i / 64, c = i % 64;
+      if (c < nk) s_t[r * 65 + c] = src[(size_t)r * ld + kb + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nk * rows; i += 256) {
+      const int e = i / rows, r = i % rows;
+      dst[(size_t)(kb + e) * rows + r] = s_t[r * 65 + e];
+    }
+  } else {
+    for (int i = threadIdx.x; i < nk * rows; i += 256) {
+      const int e = i / rows, r = i % rows;
+      s_t[r * 65 + e] = src[(size_t)(kb + e) * rows + r];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * 64; i += 256) {
+      const int r = i / 64, c = i % 64;
+      if (c < nk) dst[(size_t)r * ld + kb + c] = s_t[r * 65 + c];
+    }
+  }
+}
+
+cudaError_t launch_nm_to_em(const double* nm, double* em, int ld, int rows, int k0, int k1, cudaStream_t s) {
+  if (k1 <= k0 || rows <= 0) return cudaSuccess;
+  k_transpose_nm<true><<<(k1 - k0 + 63) / 64, 256, (size_t)rows * 65 * sizeof(double), s>>>(nm, em, ld, rows, k0, k1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_em_to_nm(const double* em, double* nm, int ld, int rows, int k0, int k1, cudaStream_t s) {
+  if (k1 <= k0 || rows <= 0) return cudaSuccess;
+  k_transpose_nm<false><<<(k1 - k0 + 63) / 64, 256, (size_t)rows * 65 * sizeof(double), s>>>(em, nm, ld, rows, k0, k1);
+  return cudaGetLastError();
+}
+
 
 int apply_grid(int K) { return (K + 127) / 128; }
 int cg_grid(int K) { return (K + 127) / 128; }

@@ -34,6 +34,7 @@ struct ApplyArgs {
   const T* kappa;           // per-element diffusivity (null: 1)
   const double* dm_img;     // float64: FP64 tensor-core operand image (null: CUDA cores)
   const double* dm_geo;     // float64: that kernel's element and face coefficients ([D_COUNT][ldg])
+  int k_lo, k_hi;           // AM_APPLY: elements [k_lo, k_hi) only (k_hi = 0: all; k_lo a multiple of 16)
 };
 
 template <typename T>
@@ -146,6 +147,10 @@ cudaError_t launch_apply_dm(int N, int mode, const ApplyArgs<double>& a, cudaStr
 // node-major (Np, K) fields, elements [k_begin, k_end) only (in0 -> out0)
 template <typename T>
 cudaError_t launch_apply_nm(int N, const ApplyArgs<T>& a, int k_begin, int k_end, cudaStream_t s);
+// node-major (rows, ld) <-> element-major (ld, rows) float64 for elements
+// [k0, k1), through shared-memory tiles
+cudaError_t launch_nm_to_em(const double* nm, double* em, int ld, int rows, int k0, int k1, cudaStream_t s);
+cudaError_t launch_em_to_nm(const double* em, double* nm, int ld, int rows, int k0, int k1, cudaStream_t s);
 template <typename T>
 cudaError_t launch_cg_step(int N, bool pc, bool init, const CgArgs<T>& a, cudaStream_t s);
 cudaError_t launch_block_jacobi(int N, const BlockArgs& a, cudaStream_t s);
