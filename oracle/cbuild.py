@@ -93,6 +93,20 @@ def _bench_mesh(Kx, Ky, N, tau_scale, alpha):
     return _CACHE[key]
 
 
+def apply_stepper(Kx, Ky, N, tau_scale, alpha):
+    """One timed float64 apply per call on all host cores (the reference arm
+    of the benchmark); returns (step() -> seconds, DOFs, threads)."""
+    op = _bench_mesh(Kx, Ky, N, tau_scale, alpha)
+    u = np.random.default_rng(1).standard_normal(op.n)
+    nt = len(os.sched_getaffinity(0))
+
+    def step():
+        t0 = time.perf_counter()
+        op(u, nt)
+        return time.perf_counter() - t0
+    return step, op.n, nt
+
+
 def time_apply(Kx, Ky, N, tau_scale, alpha, budget_s=15.0, reps=None):
     """Median time of the C+OpenMP float64 apply on all host cores."""
     op = _bench_mesh(Kx, Ky, N, tau_scale, alpha)
