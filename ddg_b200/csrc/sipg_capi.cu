@@ -11,6 +11,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ddg_sipg.h"
@@ -673,6 +674,22 @@ bool host_pinned(const void* p) {
 
 namespace {
 
+// memcpy split over a few host threads (staging of pageable arrays: one
+// thread moves far less than the memory bandwidth)
+void par_copy(void* dst, const void* src, size_t bytes) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, bytes >> 21));
+  const size_t piece = (bytes + nt - 1) / nt;
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nt; ++t) {
+    const size_t o = t * piece;
+    if (o >= bytes) break;
+    pool.emplace_back([=] { std::memcpy((char*)dst + o, (const char*)src + o, std::min(piece, bytes - o)); });
+  }
+  std::memcpy(dst, src, std::min(piece, bytes));
+  for (auto& th : pool) th.join();
+}
+
 // Issue the chunked pipeline for pinned (or staged) host arrays src -> dst
 // after the work already queued on `us`, and join it back into `us`.  Per
 // element chunk: a pitched copy engine transfer of the chunk's Np row
@@ -680,10 +697,8 @@ namespace {
 // transpose to the element-major layout in device memory, the element-major
 // apply of every chunk whose neighbours have all arrived (the tensor-core
 // kernel for float64 where built), the transpose back and the pitched copy
-// to the host.  With stage_u, chunk c of the pageable input u is first
-// copied into the pinned staging buffer (host memcpy; not capturable).
-int hio_issue(ddg_sipg_op* op, double alpha, const double* u, const double* src, double* dst, bool stage_u,
-              cudaStream_t us) {
+// to the host.  src and dst are pinned host arrays.
+int hio_issue(ddg_sipg_op* op, double alpha, const double* src, double* dst, cudaStream_t us) {
   HostIO* h = op->hio;
   const int K = op->K, Np = op->Np;
   const size_t pitch = (size_t)K * sizeof(double);
@@ -698,8 +713,6 @@ int hio_issue(ddg_sipg_op* op, double alpha, const double* u, const double* src,
   for (int c = 0; c < h->nch; ++c) {
     const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
     const size_t w = (size_t)(c1 - c0) * sizeof(double);
-    if (stage_u)  // stage this chunk while the previous one is in flight
-      for (int i = 0; i < Np; ++i) std::memcpy(h->h_u + (size_t)i * K + c0, u + (size_t)i * K + c0, w);
     CK(cudaMemcpy2DAsync(h->d_u + c0, pitch, src + c0, pitch, w, Np, cudaMemcpyHostToDevice, h->s_in));
     CK(cudaEventRecord(h->e_in[c], h->s_in));
     CK(cudaStreamWaitEvent(h->s_cmp, h->e_in[c], 0));
@@ -736,7 +749,7 @@ int hio_capture(ddg_sipg_op* op, double alpha, const double* u, double* y) {
   h->gexec = nullptr;
   h->g_ok = false;
   CK(cudaStreamBeginCapture(h->s_org, cudaStreamCaptureModeThreadLocal));
-  const int rc = hio_issue(op, alpha, u, u, y, false, h->s_org);
+  const int rc = hio_issue(op, alpha, u, y, h->s_org);
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(h->s_org, &g);
   if (rc != DDG_OK) {
@@ -770,33 +783,20 @@ extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* 
   const size_t bytes = (size_t)K * Np * sizeof(double);
   const bool u_pin = host_pinned(u), y_pin = host_pinned(y);
   cudaStream_t us = (cudaStream_t)stream;
-  if (u_pin && y_pin) {
-    // one graph launch replays the whole pipeline for these arrays
-    if (!(h->g_ok && h->g_u == u && h->g_y == y && h->g_alpha == alpha)) {
-      rc = hio_capture(op, alpha, u, y);
-      if (rc != DDG_OK) return rc;
-    }
-    CK(cudaGraphLaunch(h->gexec, us));
-    CK(cudaStreamSynchronize(us));
-    return DDG_OK;
-  }
+  // pageable arrays go through the pinned staging buffers (multi-threaded
+  // host copies); the pinned arrays' pipeline is replayed from a graph
   if (!u_pin && !h->h_u) CK(cudaMallocHost((void**)&h->h_u, bytes));
   if (!y_pin && !h->h_y) CK(cudaMallocHost((void**)&h->h_y, bytes));
   const double* src = u_pin ? u : h->h_u;
   double* dst = y_pin ? y : h->h_y;
-  rc = hio_issue(op, alpha, u, src, dst, !u_pin, us);
-  if (rc != DDG_OK) return rc;
-  if (!y_pin) {
-    for (int j = 0; j < 2 * h->nch; ++j) {
-      const int j0 = h->p_lo[j], j1 = h->p_hi[j];
-      if (j1 <= j0) continue;
-      CK(cudaEventSynchronize(h->e_out[j]));
-      for (int i = 0; i < Np; ++i)
-        std::memcpy(y + (size_t)i * K + j0, h->h_y + (size_t)i * K + j0, (size_t)(j1 - j0) * sizeof(double));
-    }
-  } else {
-    CK(cudaStreamSynchronize(us));
+  if (!u_pin) par_copy(h->h_u, u, bytes);
+  if (!(h->g_ok && h->g_u == src && h->g_y == dst && h->g_alpha == alpha)) {
+    rc = hio_capture(op, alpha, src, dst);
+    if (rc != DDG_OK) return rc;
   }
+  CK(cudaGraphLaunch(h->gexec, us));
+  CK(cudaStreamSynchronize(us));
+  if (!y_pin) par_copy(y, h->h_y, bytes);
   return DDG_OK;
 }
 

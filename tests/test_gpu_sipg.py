@@ -304,7 +304,7 @@ def test_full_size_operator_symmetry_and_linearity():
 
 
 @pytest.mark.parametrize("shuffle", [False, True])
-@pytest.mark.parametrize("Kx,Ky,N", [(64, 64, 4), (96, 48, 3)])
+@pytest.mark.parametrize("Kx,Ky,N", [(64, 64, 4), (96, 48, 3), (67, 65, 4), (37, 23, 2)])
 def test_apply_host_chunked_pipeline(Kx, Ky, N, shuffle):
     """Host-buffer apply (chunked copy / apply / copy-back on three streams)
     gives identical results on every call and matches the device apply and
