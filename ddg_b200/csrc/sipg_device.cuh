@@ -58,6 +58,19 @@ struct RefMats {
 // specialises CRef for every built degree.
 template <int N, typename T> struct CRef;
 
+// float32 operator: the reference matrices paired for the packed FP32 FMA
+// of sm_100 (__ffma2_rn, two independent accumulations per instruction):
+//   DrDs[i Np + j]  = (Dr[i][j], Ds[i][j])   gradient rows
+//   DrDsT[i Np + j] = (Dr[j][i], Ds[j][i])   lift (transposed) rows
+//   MP[r Np + j]    = (M[2r][j], M[2r+1][j]) mass rows in pairs
+template <int N>
+struct RefPairs {
+  float2 DrDs[Dim<N>::Np * Dim<N>::Np];
+  float2 DrDsT[Dim<N>::Np * Dim<N>::Np];
+  float2 MP[(Dim<N>::Np / 2) * Dim<N>::Np + 1];
+};
+template <int N> struct CPairs;
+
 // Symmetric packed index of (i, j), upper triangle (block-Jacobi inverses
 // are stored as Np (Np + 1) / 2 entries per element).
 __host__ __device__ constexpr int sym_idx(int Np, int i, int j) {
@@ -279,6 +292,12 @@ struct NbrZero {  // self-block extraction: the neighbour carries no value
   }
 };
 
+template <int N, bool USE_NBR, class NbrSrc>
+__device__ __forceinline__ void elem_apply_f2(const float (&u)[Dim<N>::Np], float (&y)[Dim<N>::Np],
+                                              const Geo<float>& g, const uint32_t (&w)[3],
+                                              const float* __restrict__ geo, int ldg, float tau, float alpha,
+                                              const NbrSrc& nbr, const float* __restrict__ kappa, int k);
+
 // y = A u + alpha J M u  for element k (u, y in registers).
 // USE_NBR=false skips the neighbour value gather (self-block mode: the
 // neighbour's value is zero, its geometry still sets tau_P).
@@ -292,6 +311,10 @@ __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<
                                            const uint32_t (&w)[3], const T* __restrict__ geo, int ldg, T tau,
                                            T alpha, const NbrSrc& nbr, const T* __restrict__ kappa = nullptr,
                                            int k = 0) {
+  if constexpr (sizeof(T) == 4) {
+    elem_apply_f2<N, USE_NBR>(u, y, g, w, geo, ldg, tau, alpha, nbr, kappa, k);
+    return;
+  }
   constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
   const RefMats<N, T>& R = CRef<N, T>::get();
   const T kM = kappa ? __ldg(kappa + k) : T(1);
@@ -451,6 +474,162 @@ __device__ __forceinline__ void elem_apply(const T (&u)[Dim<N>::Np], T (&y)[Dim<
       a = fma(R.Ds[j * Np + i], ts[j], a);
     }
     y[i] = a;
+  }
+}
+
+
+// float32 version of elem_apply with paired accumulations (same terms and
+// coefficients; every component follows the scalar FMA sequence except the
+// lift, which sums its Dr and Ds parts in two accumulators).
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <int N, bool USE_NBR, class NbrSrc>
+__device__ __forceinline__ void elem_apply_f2(const float (&u)[Dim<N>::Np], float (&y)[Dim<N>::Np],
+                                              const Geo<float>& g, const uint32_t (&w)[3],
+                                              const float* __restrict__ geo, int ldg, float tau, float alpha,
+                                              const NbrSrc& nbr, const float* __restrict__ kappa, int k) {
+  constexpr int Np = Dim<N>::Np, Nfp = Dim<N>::Nfp;
+  const RefMats<N, float>& R = CRef<N, float>::get();
+  const RefPairs<N>& P = CPairs<N>::get();
+  const float kM = kappa ? __ldg(kappa + k) : 1.0f;
+
+  // physical gradient at the nodes: (ux, uy)
+  float2 uxy[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    float2 a = f2(0.f, 0.f);  // (Dr u, Ds u)_i
+#pragma unroll
+    for (int j = 0; j < Np; ++j) a = __ffma2_rn(P.DrDs[i * Np + j], f2(u[j], u[j]), a);
+    uxy[i] = f2(g.rx * a.x + g.sx * a.y, g.ry * a.x + g.sy * a.y);
+  }
+  float dnm[3][Nfp];
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const int n = fmask_idx(N, f, p);
+      dnm[f][p] = g.nx[f] * uxy[n].x + g.ny[f] * uxy[n].y;
+    }
+  // (ex, ey) = M^T (J ux, J uy)
+  float2 exy[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    float2 a = f2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      const float m = R.M[j * Np + i];
+      a = __ffma2_rn(f2(m, m), uxy[j], a);
+    }
+    exy[i] = f2(kM * g.J * a.x, kM * g.J * a.y);
+  }
+  // mass term (Helmholtz): alpha J (M u), rows in pairs
+#pragma unroll
+  for (int i = 0; i < Np; ++i) y[i] = 0.f;
+  if (alpha != 0.f) {
+#pragma unroll
+    for (int r = 0; r < Np / 2; ++r) {
+      float2 a = f2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < Np; ++j) a = __ffma2_rn(P.MP[r * Np + j], f2(u[j], u[j]), a);
+      y[2 * r] = alpha * g.J * a.x;
+      y[2 * r + 1] = alpha * g.J * a.y;
+    }
+    if (Np % 2) {
+      float a = 0.f;
+#pragma unroll
+      for (int j = 0; j < Np; ++j) a = fmaf(R.M[(Np - 1) * Np + j], u[j], a);
+      y[Np - 1] = alpha * g.J * a;
+    }
+  }
+  // faces
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const uint32_t wf = w[f];
+    const int bc = (wf >> 3) & 3;
+    const bool pact = (wf >> 5) & 1;
+    const bool mint = (wf >> 6) & 1;
+    const bool mdir = (bc == 1);
+    if (!(pact || mint || mdir)) continue;
+    const float sJ = g.sJ[f], nx = g.nx[f], ny = g.ny[f];
+    const float tauM = tau * sJ / g.J;
+    float uP[Nfp], dnP[Nfp];
+    float tauP = tauM;
+    float kP = kM;
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      uP[p] = 0.f;
+      dnP[p] = 0.f;
+    }
+    if (pact || mint) {
+      const int kp = (int)(wf >> 7), fp = (int)(wf & 3);
+      const bool flip = (wf >> 2) & 1;
+      if (kappa) kP = __ldg(kappa + kp);
+      const float rxn = __ldg(geo + G_RX * ldg + kp), sxn = __ldg(geo + G_SX * ldg + kp);
+      const float ryn = __ldg(geo + G_RY * ldg + kp), syn = __ldg(geo + G_SY * ldg + kp);
+      const float Jn = __ldg(geo + G_J * ldg + kp);
+      tauP = tau * sJ / Jn;
+      if (USE_NBR) {
+        float ut[Np];
+        nbr(kp, fp, ut);
+        const float ar = nx * rxn + ny * ryn, as = nx * sxn + ny * syn;
+        const float cr = fp == 0 ? ar : (fp == 1 ? as : -ar - as);
+        const float cs = fp == 0 ? as : (fp == 1 ? -ar - as : ar);
+        float dq[Nfp];
+#pragma unroll
+        for (int q = 0; q < Nfp; ++q) {
+          float2 a = f2(0.f, 0.f);  // face-0 rows: fmask_idx(N,0,q) == q
+#pragma unroll
+          for (int j = 0; j < Np; ++j) a = __ffma2_rn(P.DrDs[q * Np + j], f2(ut[j], ut[j]), a);
+          dq[q] = cr * a.x + cs * a.y;
+        }
+#pragma unroll
+        for (int p = 0; p < Nfp; ++p) {
+          uP[p] = flip ? ut[N - p] : ut[p];
+          dnP[p] = flip ? dq[N - p] : dq[p];
+        }
+      }
+    }
+    const float kF = kappa ? 0.5f * (kM + kP) : 1.0f;
+    const float caM = mdir ? 1.f : (mint ? 0.5f : 0.f);
+    const float cjM = mdir ? (kappa ? tauM * kM : tauM) : (mint ? (kappa ? 0.5f * tauM * kF : 0.5f * tauM) : 0.f);
+    const float cgM = (mdir ? 1.f : (mint ? 0.25f : 0.f)) * kM;
+    const float caP = pact ? 0.5f : 0.f;
+    const float cjP = pact ? (kappa ? 0.5f * tauP * kF : 0.5f * tauP) : 0.f;
+    const float cgP = (pact ? 0.25f : 0.f) * kM;
+    float2 v12[Nfp];
+#pragma unroll
+    for (int p = 0; p < Nfp; ++p) {
+      const float uM = u[fmask_idx(N, f, p)];
+      const float avgI = kappa ? 0.5f * (kM * dnm[f][p] + kP * dnP[p]) : 0.5f * (dnm[f][p] + dnP[p]);
+      const float jmpI = uM - uP[p];
+      const float avgM = mdir ? (kappa ? kM * dnm[f][p] : dnm[f][p]) : avgI;
+      const float jmpM = mdir ? uM : jmpI;
+      v12[p] = f2(-caM * avgM + cjM * jmpM - caP * avgI + cjP * jmpI, cgM * jmpM + cgP * jmpI);
+    }
+#pragma unroll
+    for (int q = 0; q < Nfp; ++q) {
+      float2 a = f2(0.f, 0.f);
+#pragma unroll
+      for (int p = 0; p < Nfp; ++p) {
+        const float m = R.m1d[(f * Nfp + p) * Nfp + q];
+        a = __ffma2_rn(f2(m, m), v12[p], a);
+      }
+      const int n = fmask_idx(N, f, q);
+      y[n] += sJ * a.x;
+      exy[n].x -= sJ * nx * a.y;
+      exy[n].y -= sJ * ny * a.y;
+    }
+  }
+  // lift: y += Dr^T (rx ex + ry ey) + Ds^T (sx ex + sy ey)
+  float2 trs[Np];
+#pragma unroll
+  for (int i = 0; i < Np; ++i) trs[i] = f2(g.rx * exy[i].x + g.ry * exy[i].y, g.sx * exy[i].x + g.sy * exy[i].y);
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+    float2 a = f2(y[i], 0.f);
+#pragma unroll
+    for (int j = 0; j < Np; ++j) a = __ffma2_rn(P.DrDsT[i * Np + j], trs[j], a);
+    y[i] = a.x + a.y;
   }
 }
 

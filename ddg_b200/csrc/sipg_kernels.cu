@@ -15,7 +15,8 @@ namespace ddg {
 
 #define DDG_DEFINE_CONST(NN)                       \
   __constant__ RefMats<NN, double> c_ref64_##NN; \
-  __constant__ RefMats<NN, float> c_ref32_##NN;
+  __constant__ RefMats<NN, float> c_ref32_##NN;  \
+  __constant__ RefPairs<NN> c_pair32_##NN;
 DDG_DEFINE_CONST(1)
 DDG_DEFINE_CONST(2)
 DDG_DEFINE_CONST(3)
@@ -34,6 +35,16 @@ DDG_CREF(2)
 DDG_CREF(3)
 DDG_CREF(4)
 DDG_CREF(5)
+
+#define DDG_CPAIRS(NN)                                                                   \
+  template <> struct CPairs<NN> {                                                      \
+    static __device__ __forceinline__ const RefPairs<NN>& get() { return c_pair32_##NN; } \
+  };
+DDG_CPAIRS(1)
+DDG_CPAIRS(2)
+DDG_CPAIRS(3)
+DDG_CPAIRS(4)
+DDG_CPAIRS(5)
 
 // ================================================================ apply
 // MODE: AM_APPLY  out0 = A in0 + alpha J M in0 + shift in0
@@ -935,6 +946,14 @@ DDG_SYM(2)
 DDG_SYM(3)
 DDG_SYM(4)
 DDG_SYM(5)
+template <int N> struct CPairSym;
+#define DDG_PSYM(NN) \
+  template <> struct CPairSym<NN> { static const void* sym() { return &c_pair32_##NN; } };
+DDG_PSYM(1)
+DDG_PSYM(2)
+DDG_PSYM(3)
+DDG_PSYM(4)
+DDG_PSYM(5)
 
 namespace {
 template <int N, typename T>
@@ -947,7 +966,18 @@ cudaError_t upload_one(const double* Dr, const double* Ds, const double* M, cons
     h.M[i] = (T)M[i];
   }
   for (int i = 0; i < 3 * Nfp * Nfp; ++i) h.m1d[i] = (T)m1d[i];
-  return cudaMemcpyToSymbol(CRefSym<N, T>::sym(), &h, sizeof(h));
+  cudaError_t e = cudaMemcpyToSymbol(CRefSym<N, T>::sym(), &h, sizeof(h));
+  if (e != cudaSuccess || sizeof(T) != 4) return e;
+  RefPairs<N> pr{};
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) {
+      pr.DrDs[i * Np + j] = make_float2((float)Dr[i * Np + j], (float)Ds[i * Np + j]);
+      pr.DrDsT[i * Np + j] = make_float2((float)Dr[j * Np + i], (float)Ds[j * Np + i]);
+    }
+  for (int r = 0; r < Np / 2; ++r)
+    for (int j = 0; j < Np; ++j)
+      pr.MP[r * Np + j] = make_float2((float)M[2 * r * Np + j], (float)M[(2 * r + 1) * Np + j]);
+  return cudaMemcpyToSymbol(CPairSym<N>::sym(), &pr, sizeof(pr));
 }
 }  // namespace
 
