@@ -233,6 +233,7 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
 
   if (MODE == AM_PFUSE && a.ctl->cont == 0) return;  // the loop has stopped (uniform)
   const RefMats<N, float>& R = CRef<N, float>::get();
+  const RefPairs<N>& P = CPairs<N>::get();
   const int tid = threadIdx.x, warp = tid >> 5;
   const int ntiles = (a.K + 127) / 128;
   const float beta = (MODE == AM_PFUSE) ? (float)a.ctl->beta : 0.0f;
@@ -367,13 +368,10 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
         float dq[Nfp];
 #pragma unroll
         for (int q = 0; q < Nfp; ++q) {
-          float s1f = 0.0f, s2f = 0.0f;
+          float2 s = make_float2(0.0f, 0.0f);  // (Dr_F0 u~, Ds_F0 u~), packed FP32 FMA
 #pragma unroll
-          for (int j = 0; j < Np; ++j) {
-            s1f = fmaf(R.Dr[q * Np + j], ut[j], s1f);
-            s2f = fmaf(R.Ds[q * Np + j], ut[j], s2f);
-          }
-          dq[q] = cr * s1f + cs * s2f;
+          for (int j = 0; j < Np; ++j) s = __ffma2_rn(P.DrDs[q * Np + j], make_float2(ut[j], ut[j]), s);
+          dq[q] = cr * s.x + cs * s.y;
         }
 #pragma unroll
         for (int p = 0; p < Nfp; ++p) {
@@ -458,12 +456,13 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
       }
 #pragma unroll
       for (int q = 0; q < Nfp; ++q) {
-        float s1f = 0.0f, s2f = 0.0f;
+        float2 s = make_float2(0.0f, 0.0f);  // the face mass on both flux vectors, packed FP32 FMA
 #pragma unroll
         for (int p = 0; p < Nfp; ++p) {
-          s1f = fmaf(R.m1d[(f * Nfp + p) * Nfp + q], v1[p], s1f);
-          s2f = fmaf(R.m1d[(f * Nfp + p) * Nfp + q], v2[p], s2f);
+          const float m = R.m1d[(f * Nfp + p) * Nfp + q];
+          s = __ffma2_rn(make_float2(m, m), make_float2(v1[p], v2[p]), s);
         }
+        const float s1f = s.x, s2f = s.y;
         y[fmask_idx(N, f, q)] += sJ * s1f;
         a2[f * Nfp + q] = -sJ * arM * s2f;
         a2[3 * Nfp + f * Nfp + q] = -sJ * asM * s2f;
