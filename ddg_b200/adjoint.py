@@ -33,26 +33,28 @@ def _cg(op, b, tol, maxiter):
 
 class _KappaState:
     """Keeps the handle's diffusivity and preconditioner in sync with the
-    kappa a forward or backward pass needs."""
+    kappa a forward or backward pass needs.  Stored on the operator itself,
+    so it lives exactly as long as the handle (no module-level registry
+    keeps operators alive)."""
 
-    def __init__(self, op: SipgOperator):
-        self.op = op
+    def __init__(self):
         self.current = None
 
-    def use(self, kappa):
+    def use(self, op: SipgOperator, kappa):
         if self.current is None or not np.array_equal(self.current, kappa):
-            self.op.set_kappa(kappa)
-            self.op.pc_build(0.0)
+            self.op_set(op, kappa)
             self.current = kappa.copy()
 
-
-_STATES: dict = {}
+    @staticmethod
+    def op_set(op, kappa):
+        op.set_kappa(kappa)
+        op.pc_build(0.0)
 
 
 def _state(op):
-    s = _STATES.get(id(op))
-    if s is None or s.op is not op:
-        s = _STATES[id(op)] = _KappaState(op)
+    s = getattr(op, "_kappa_state", None)
+    if s is None:
+        s = op._kappa_state = _KappaState()
     return s
 
 
@@ -76,7 +78,7 @@ def _torch_fn():
             kappa = torch.exp(g)
             k_np = kappa.detach().cpu().numpy()
             st = _state(op)
-            st.use(k_np)
+            st.use(op, k_np)
             u, _ = _cg(op, mass_apply(op, f.detach().contiguous()), tol, maxiter)
             ctx.op, ctx.tol, ctx.maxiter, ctx.k_np = op, tol, maxiter, k_np
             ctx.save_for_backward(u, kappa)
@@ -86,7 +88,7 @@ def _torch_fn():
         def backward(ctx, gu):
             u, kappa = ctx.saved_tensors
             op = ctx.op
-            _state(op).use(ctx.k_np)
+            _state(op).use(op, ctx.k_np)
             lam, _ = _cg(op, gu.contiguous(), ctx.tol, ctx.maxiter)
             gk = op.grad_kappa(u, lam)
             return -gk * kappa, mass_apply(op, lam), None, None, None
@@ -118,7 +120,7 @@ def loss_and_grad(op, g_batch, f, u_obs, tol=1e-12, maxiter=20000):
     its = 0
     for i in range(B):
         kappa = torch.exp(g_batch[i])
-        st.use(kappa.cpu().numpy())
+        st.use(op, kappa.cpu().numpy())
         u, i1 = _cg(op, b, tol, maxiter)
         r = u.clone()
         axpby(-1.0, u_obs, 1.0, r)
@@ -134,7 +136,7 @@ def loss_only(op, g, f, u_obs, tol=1e-13, maxiter=40000):
     """L for one kappa = exp(g) (the finite-difference check's evaluations)."""
     import torch
     st = _state(op)
-    st.use(torch.exp(g).cpu().numpy())
+    st.use(op, torch.exp(g).cpu().numpy())
     u, _ = _cg(op, mass_apply(op, f), tol, maxiter)
     r = u.clone()
     axpby(-1.0, u_obs, 1.0, r)

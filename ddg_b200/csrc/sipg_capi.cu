@@ -150,8 +150,11 @@ struct ddg_sipg_op {
   double* dm_img = nullptr;         // FP64 tensor-core (DMMA) B operands of this degree (device)
   double* dm_geo = nullptr;         // that kernel's element and face coefficients (device)
   int fp64_engine = DDG_ENGINE_TENSOR_CORES;   // every float64 apply (stand-alone, CG, residuals)
-
+  std::vector<ddg_mg*> mgs;         // multigrid objects whose V-cycle is embedded in this handle's CG graphs
 };
+
+// Defined after struct ddg_mg: removes op from mg's list of graph holders.
+static void mg_forget_user(ddg_mg* mg, ddg_sipg_op* op);
 
 namespace {
 
@@ -341,6 +344,8 @@ int get_graph(ddg_sipg_op* op, const GraphKey& key, CgGraph** out) {
 }
 
 void free_op(ddg_sipg_op* op) {
+  for (ddg_mg* mg : op->mgs) mg_forget_user(mg, op);   // the multigrid must not reach this handle again
+  op->mgs.clear();
   for (auto& kv : op->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.g) cudaGraphDestroy(kv.second.g);
@@ -353,7 +358,7 @@ void free_op(ddg_sipg_op* op) {
   if (op->dm_img) cudaFree(op->dm_img);
   if (op->dm_geo) cudaFree(op->dm_geo);
 
-  void* ptrs[] = {op->kappa64, op->kappa32, op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
+  void* ptrs[] = {op->kappa64 /* kappa32 lives in the same block */, op->geo64, op->geo32, op->nbr, op->perm, op->status, op->ctl, op->partA, op->partB, op->partC,
                   op->ticket, op->dotbuf, op->blocks, op->binv64, op->binv32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -802,6 +807,8 @@ extern "C" int ddg_sipg_apply_host(ddg_sipg_op* op, double alpha, const double* 
 
 extern "C" int ddg_sipg_set_engine(ddg_sipg_op* op, int engine) {
   if (!op) return fail(DDG_ERR_INVALID, "ddg_sipg_set_engine: null handle");
+  // The captured host-buffer pipeline baked in the previous engine's kernel.
+  if (op->hio) op->hio->g_ok = false;
   if (engine == DDG_ENGINE_CUDA_CORES) {
     op->fp32_engine = op->cg32_engine = op->fp64_engine = engine;
     return DDG_OK;
@@ -1176,6 +1183,7 @@ struct ddg_mg {
     void *x = nullptr, *t = nullptr, *b = nullptr, *r = nullptr;
     void *P = nullptr, *R = nullptr;          // prolongation / restriction (MG precision)
   };
+
   std::vector<Lv> lv;
   void* Ainv = nullptr;
   int nc = 0;
@@ -1183,6 +1191,10 @@ struct ddg_mg {
   double *spa = nullptr, *spb = nullptr;
   std::vector<ddg_sipg_op*> users;           // handles holding CG graphs that embed this V-cycle
 };
+
+static void mg_forget_user(ddg_mg* mg, ddg_sipg_op* op) {
+  mg->users.erase(std::remove(mg->users.begin(), mg->users.end(), op), mg->users.end());
+}
 
 namespace {
 
@@ -1385,6 +1397,7 @@ int get_mg_graph(ddg_sipg_op* op, ddg_mg* mg, const GraphKey& key, CgGraph** out
   op->mg_graphs[k2] = cg;
   *out = &op->mg_graphs[k2];
   if (std::find(mg->users.begin(), mg->users.end(), op) == mg->users.end()) mg->users.push_back(op);
+  if (std::find(op->mgs.begin(), op->mgs.end(), mg) == op->mgs.end()) op->mgs.push_back(mg);
   return DDG_OK;
 }
 
@@ -1449,7 +1462,9 @@ extern "C" int ddg_mg_destroy(ddg_mg* mg) {
         ++it;
       }
     }
+    op->mgs.erase(std::remove(op->mgs.begin(), op->mgs.end(), mg), op->mgs.end());
   }
+  mg->users.clear();
   mg_free(mg);
   return DDG_OK;
 }
@@ -1548,9 +1563,14 @@ extern "C" int ddg_sipg_set_kappa(ddg_sipg_op* op, const double* kappa) {
     for (int k = 0; k < op->K; ++k)
       if (!(kappa[k] > 0.0) || !std::isfinite(kappa[k]))
         return fail(DDG_ERR_INVALID, "ddg_sipg_set_kappa: diffusivity must be positive and finite");
-    if (!op->kappa64) {
-      CK(cudaMalloc((void**)&op->kappa64, (size_t)op->K * 8));
-      CK(cudaMalloc((void**)&op->kappa32, (size_t)op->K * 4));
+    if (!op->kappa64 || !op->kappa32) {       // one block: both copies or neither
+      if (op->kappa64) cudaFree(op->kappa64);
+      op->kappa64 = nullptr;
+      op->kappa32 = nullptr;
+      void* blk = nullptr;
+      CK(cudaMalloc(&blk, (size_t)op->K * 8 + (size_t)op->K * 4 + 16));
+      op->kappa64 = (double*)blk;
+      op->kappa32 = (float*)((char*)blk + (((size_t)op->K * 8 + 15) & ~(size_t)15));
     }
     std::vector<float> k32(kappa, kappa + op->K);
     CK(cudaDeviceSynchronize());

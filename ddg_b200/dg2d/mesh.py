@@ -112,7 +112,10 @@ class Mesh2D:
         if op is None:
             op = SipgOperator(self, bc, tau_scale=tau_scale, device=dev)
             while len(self._ops) >= 4:
-                self._ops.pop(next(iter(self._ops))).close()
+                # drop only the cache's reference: a preconditioner or caller
+                # may still hold the operator; its handle is freed with the
+                # last reference
+                self._ops.pop(next(iter(self._ops)))
         self._ops[key] = op            # most recently used last
         return op
 

@@ -58,6 +58,7 @@ class SipgOperator:
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.lib().ddg_sipg_destroy(self._h)
             self._h = None
+        self._kappa_state = None
 
     def __del__(self):
         try:

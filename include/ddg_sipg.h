@@ -112,7 +112,9 @@ int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
  * cores; float32 CG iterations (ddg_sipg_cg with DDG_FP32,
  * ddg_sipg_cg_mixed) the CUDA cores, whose restarted mixed-precision
  * iterations converge in fewer steps.  Calling this sets all three where
- * the degree has the engine (DDG_ERR_UNSUPPORTED if it has none).  No
+ * the degree has the engine (DDG_ERR_UNSUPPORTED if it has none); the
+ * float32 CG default is not restored by a later call.  The host-buffer
+ * apply recaptures its pipeline with the new engine on its next call.  No
  * reference counterpart (the reference's operator is jax.grad of its
  * bilinear form, sipg.py:304-337). */
 #define DDG_ENGINE_CUDA_CORES   0

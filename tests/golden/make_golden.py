@@ -1,0 +1,268 @@
+"""Generate golden fixtures from the UNMODIFIED reference (ddg) for the SIPG path.
+
+TEST INFRASTRUCTURE ONLY.  Run here, where the reference sources are present::
+
+    python tests/golden/make_golden.py [/path/to/ddg/src]
+
+(default source path: ``/root/reference/src``).  The reference's own modules
+``ddg.dg1d.reference``, ``ddg.dg2d.reference``, ``ddg.dg2d.mesh``,
+``ddg.dg2d.sipg``, ``ddg.dg2d.multigrid`` and ``ddg.dg2d.refinement`` are
+imported unchanged over the numpy-backed JAX stand-in in ``refshim.py``
+(JAX itself cannot be installed in this container).  Every number written
+here is computed by the reference's code path:
+
+* reference elements N = 1..6: ``equilateral_nodes_2d``, ``vandermonde_2d``,
+  ``d_matrices_2d``, ``lift_2d``, ``face_masks_2d`` through ``build_mesh_2d``,
+  plus ``sipg._local_mass`` and ``sipg._face_1d_mass_matrices``;
+* meshes: ``uniform_rectangle_mesh_2d`` + ``build_mesh_2d`` (connectivity,
+  node maps, geometric factors, normals), a vertex-perturbed mesh with
+  shuffled element order, and a ``RefinementForest`` hierarchy;
+* operator applies: ``sipg_apply_2d`` (``jax.grad`` of ``sipg_bilinear_form``)
+  for random ``u`` under several boundary-condition sets and penalties, with
+  and without ``u_dir``; the dense ``sipg_matrix_2d`` and
+  ``sipg_helmholtz_matrix_2d`` of a tiny mesh;
+* loads: ``sipg_dirichlet_load_2d`` and ``sipg_neumann_load_2d``;
+* block diagonals: ``extract_block_diag_matfree`` and ``_color_elements``;
+* solves: ``solve_sipg_poisson_2d`` by matrix-free CG and by dense LU on the
+  plain manufactured-solution workload (12 x 12 quads, N = 4,
+  ``tau_scale = 0.5``), the singular (all-Neumann) branch with its epsilon
+  shift, ``solve_sipg_helmholtz_2d`` with the block-Jacobi preconditioner,
+  and CG preconditioned by the p- and hp-multigrid V-cycles, with the
+  iteration counts the CG loop took.
+
+Outputs: ``refelem.npz``, ``meshes.npz``, ``applies.npz``, ``solves.npz``
+next to this file.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import refshim  # noqa: E402
+
+MESH_FIELDS = ("VX", "VY", "EToV", "x", "y", "rx", "sx", "ry", "sy", "J", "nx", "ny", "sJ",
+               "Fscale", "EToE", "EToF", "vmapM", "vmapP", "vmapB", "mapB")
+
+
+def _a(x):
+    return np.asarray(x)
+
+
+def boundary_faces(m):
+    K = int(m.K)
+    return _a(m.EToE) == np.arange(K)[:, None]
+
+
+def bc_sets(m, rng):
+    """Named (K, 3) int32 boundary-condition arrays for a mesh."""
+    K = int(m.K)
+    isb = boundary_faces(m)
+    nx = _a(m.nx).reshape((int(m.Nfp), 3, K), order="F")[0].T
+    rnd = rng.integers(1, 3, size=(K, 3))
+    return {
+        "dirichlet": np.where(isb, 1, 0).astype(np.int32),
+        "neumann": np.where(isb, 2, 0).astype(np.int32),
+        "dir_x_neu_y": np.where(isb, np.where(np.abs(nx) > 0.5, 1, 2), 0).astype(np.int32),
+        "random": np.where(isb, rnd, 0).astype(np.int32),
+    }
+
+
+def main(src: str) -> None:
+    imp = refshim.install(src)
+    rmesh = imp("ddg.dg2d.mesh")
+    rsipg = imp("ddg.dg2d.sipg")
+    rmg = imp("ddg.dg2d.multigrid")
+    rref = imp("ddg.dg2d.refinement")
+    t0 = time.time()
+    out_ref, out_mesh, out_app, out_sol = {}, {}, {}, {}
+
+    # ---- reference elements
+    for N in range(1, 7):
+        VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 1, 1)
+        m = rmesh.build_mesh_2d(VX, VY, E, N)
+        for f in ("r", "s", "V", "invV", "Dr", "Ds", "LIFT", "Fmask"):
+            out_ref[f"N{N}_{f}"] = _a(getattr(m, f))
+        out_ref[f"N{N}_M"] = _a(rsipg._local_mass(m))
+        out_ref[f"N{N}_m1d"] = _a(rsipg._face_1d_mass_matrices(m))
+
+    # ---- meshes
+    meshes = {}
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 12, 12)
+    meshes["plain12_N4"] = rmesh.build_mesh_2d(VX, VY, E, 4)
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 2.0, 4, 8)
+    meshes["rect4x8_N3"] = rmesh.build_mesh_2d(VX, VY, E, 3)
+    # perturbed interior vertices + shuffled element order (seeded)
+    rng = np.random.default_rng(2024)
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 5, 5)
+    VX, VY, E = _a(VX).copy(), _a(VY).copy(), _a(E).copy()
+    inner = (VX > 1e-12) & (VX < 1 - 1e-12) & (VY > 1e-12) & (VY < 1 - 1e-12)
+    h = 1.0 / 5
+    VX[inner] += 0.2 * h * rng.uniform(-1, 1, inner.sum())
+    VY[inner] += 0.2 * h * rng.uniform(-1, 1, inner.sum())
+    E = E[rng.permutation(E.shape[0])]
+    meshes["perturbed5_N2"] = rmesh.build_mesh_2d(VX, VY, E, 2)
+    # forest refinement (leaf-ordered active mesh), 2 uniform levels on [0,1]x[0,2]
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 2.0, 2, 3)
+    base = rmesh.build_mesh_2d(VX, VY, E, 4)
+    hm = rmg._build_h_meshes(base, 2)
+    meshes["refined2x3x2_N4"] = hm[-1]
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 2, 2)
+    meshes["tiny2_N2"] = rmesh.build_mesh_2d(VX, VY, E, 2)
+    for name, m in meshes.items():
+        for f in MESH_FIELDS:
+            out_mesh[f"{name}/{f}"] = _a(getattr(m, f))
+        out_mesh[f"{name}/N"] = np.int64(m.N)
+    print(f"meshes done {time.time() - t0:.1f}s", flush=True)
+
+    # ---- applies
+    rng = np.random.default_rng(7)
+    for name, m in meshes.items():
+        sets = bc_sets(m, rng)
+        if name == "plain12_N4":
+            combos = [("dirichlet", 0.5), ("dir_x_neu_y", 0.5), ("neumann", 200.0)]
+        else:
+            combos = [(b, t) for b in sets for t in (200.0, 0.5)]
+        for bname, tau in combos:
+            bc = sets[bname]
+            u = rng.standard_normal((int(m.Np), int(m.K)))
+            y = _a(rsipg.sipg_apply_2d(m, u, bc_types=bc, tau_scale=tau))
+            key = f"{name}/{bname}/tau{tau:g}"
+            out_app[key + "/bc"] = bc
+            out_app[key + "/u"] = u
+            out_app[key + "/Au"] = y
+        # affine apply with u_dir on the Dirichlet set
+        bc = sets["dir_x_neu_y"]
+        u = rng.standard_normal((int(m.Np), int(m.K)))
+        ud = np.sin(np.pi * _a(m.x)) * np.cos(np.pi * _a(m.y))
+        y = _a(rsipg.sipg_apply_2d(m, u, bc_types=bc, u_dir=ud, tau_scale=200.0))
+        out_app[f"{name}/udir/bc"] = bc
+        out_app[f"{name}/udir/u"] = u
+        out_app[f"{name}/udir/u_dir"] = ud
+        out_app[f"{name}/udir/Au"] = y
+        # loads
+        q = rng.standard_normal((3 * int(m.Nfp), int(m.K)))
+        out_app[f"{name}/loads/bc"] = bc
+        out_app[f"{name}/loads/u_dir"] = ud
+        out_app[f"{name}/loads/q_neu"] = q
+        out_app[f"{name}/loads/LD"] = _a(rsipg.sipg_dirichlet_load_2d(m, ud, bc_types=bc, tau_scale=200.0))
+        out_app[f"{name}/loads/LN"] = _a(rsipg.sipg_neumann_load_2d(m, q, bc_types=bc))
+    print(f"applies done {time.time() - t0:.1f}s", flush=True)
+
+    # ---- dense matrices of a tiny mesh
+    m = meshes["tiny2_N2"]
+    bc = bc_sets(m, rng)["dir_x_neu_y"]
+    out_app["tiny2_N2/dense/bc"] = bc
+    out_app["tiny2_N2/dense/A"] = _a(rsipg.sipg_matrix_2d(m, bc_types=bc, tau_scale=200.0))
+    out_app["tiny2_N2/dense/H"] = _a(rsipg.sipg_helmholtz_matrix_2d(m, alpha=5.0, nu=1.0, bc_types=bc,
+                                                                    tau_scale=200.0))
+
+    # ---- block diagonals by coloured probing
+    for name in ("rect4x8_N3", "perturbed5_N2"):
+        m = meshes[name]
+        bc = bc_sets(m, rng)["dir_x_neu_y"]
+        col, ncol = rsipg._color_elements(m)
+        out_app[f"{name}/blocks/colors"] = _a(col)
+        out_app[f"{name}/blocks/ncolors"] = np.int64(ncol)
+        Np, K = int(m.Np), int(m.K)
+
+        def apply_flat(v, m=m, bc=bc):
+            return rsipg.sipg_apply_2d(m, v.reshape(K, Np).T, bc_types=bc, tau_scale=200.0).T.reshape(-1)
+        out_app[f"{name}/blocks/bc"] = bc
+        out_app[f"{name}/blocks/B"] = _a(rsipg.extract_block_diag_matfree(apply_flat, m))
+    print(f"dense + blocks done {time.time() - t0:.1f}s", flush=True)
+
+    # ---- solves
+    IC = rsipg.IterativeConfig
+    m = meshes["plain12_N4"]
+    bc = bc_sets(m, rng)["dirichlet"]
+    ue = np.sin(np.pi * _a(m.x)) * np.sin(np.pi * _a(m.y))
+    f = 2 * np.pi ** 2 * ue
+    x = rsipg.solve_sipg_poisson_2d(m, f, bc_types=bc, u_dir=ue, tau_scale=0.5, iterative=IC(tol=1e-9))
+    out_sol["plain/bc"] = bc
+    out_sol["plain/u_cg"] = _a(x)
+    out_sol["plain/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    print(f"plain CG {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+    x = rsipg.solve_sipg_poisson_2d(m, f, bc_types=bc, u_dir=ue, tau_scale=0.5)
+    out_sol["plain/u_lu"] = _a(x)
+    print(f"plain LU done {time.time() - t0:.1f}s", flush=True)
+
+    # singular all-Neumann Poisson (eps shift + mean deflation branch)
+    m = meshes["rect4x8_N3"]
+    bc = bc_sets(m, rng)["neumann"]
+    src = np.cos(np.pi * _a(m.x)) * np.cos(0.5 * np.pi * _a(m.y)) + 0.3
+    x = rsipg.solve_sipg_poisson_2d(m, src, bc_types=bc, tau_scale=200.0, iterative=IC(tol=1e-10))
+    out_sol["singular/bc"] = bc
+    out_sol["singular/source"] = src
+    out_sol["singular/u"] = _a(x)
+    out_sol["singular/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+
+    # Helmholtz, Dirichlet x / Neumann y, block-Jacobi PCG (precision workload shape, small)
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 16, 16)
+    m = rmesh.build_mesh_2d(VX, VY, E, 4)
+    bc = bc_sets(m, rng)["dir_x_neu_y"]
+    frng = np.random.default_rng(0)
+    kx = frng.integers(1, 7, 8)
+    ky = frng.integers(1, 7, 8)
+    amp = frng.standard_normal(8)
+    rhs = sum(a * np.sin(np.pi * i * _a(m.x)) * np.cos(np.pi * j * _a(m.y)) for a, i, j in zip(amp, kx, ky))
+    pc = rsipg.make_helmholtz_block_jacobi_preconditioner(m, alpha=5.0, nu=1.0, bc_types=bc, tau_scale=0.5)
+    x = rsipg.solve_sipg_helmholtz_2d(m, rhs, alpha=5.0, nu=1.0, bc_types=bc, tau_scale=0.5,
+                                      iterative=IC(tol=1e-10, maxiter=5000), preconditioner=pc)
+    out_sol["helmholtz16/bc"] = bc
+    out_sol["helmholtz16/rhs"] = rhs
+    out_sol["helmholtz16/u"] = _a(x)
+    out_sol["helmholtz16/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    print(f"helmholtz {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+
+    # p-multigrid PCG (N = 3 -> 2 -> 1) on the 4x8 rectangle, Dirichlet x / Neumann y
+    m = meshes["rect4x8_N3"]
+    bc = bc_sets(m, rng)["dir_x_neu_y"]
+    src = np.sin(np.pi * _a(m.x)) * np.cos(np.pi * _a(m.y)) + 0.5
+    pc = rmg.make_sipg_mg_preconditioner(m, bc_types=bc, tau_scale=200.0)
+    x = rsipg.solve_sipg_poisson_2d(m, src, bc_types=bc, tau_scale=200.0, iterative=IC(tol=1e-8),
+                                    preconditioner=pc)
+    out_sol["pmg/bc"] = bc
+    out_sol["pmg/source"] = src
+    out_sol["pmg/u"] = _a(x)
+    out_sol["pmg/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    r = np.random.default_rng(11).standard_normal(int(m.Np) * int(m.K))
+    out_sol["pmg/vcycle_in"] = r
+    out_sol["pmg/vcycle_out"] = _a(pc(r))
+    print(f"pmg {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+
+    # hp-multigrid PCG: base 2x4 on [0,1]x[0,2], 2 h-levels, N = 3, Dirichlet everywhere
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 2.0, 2, 4)
+    base = rmesh.build_mesh_2d(VX, VY, E, 3)
+
+    def bc_fn(mm):
+        return np.where(boundary_faces(mm), 1, 0).astype(np.int32)
+    pc, fine = rmg.make_sipg_hpmg_preconditioner(base, 2, bc_fn=bc_fn, tau_scale=200.0)
+    bc = bc_fn(fine)
+    src = np.sin(np.pi * _a(fine.x)) * np.sin(0.5 * np.pi * _a(fine.y)) * 5.0
+    x = rsipg.solve_sipg_poisson_2d(fine, src, bc_types=bc, tau_scale=200.0, iterative=IC(tol=1e-8),
+                                    preconditioner=pc)
+    for f_ in ("VX", "VY", "EToV"):
+        out_sol[f"hpmg/fine_{f_}"] = _a(getattr(fine, f_))
+    out_sol["hpmg/bc"] = bc
+    out_sol["hpmg/source"] = src
+    out_sol["hpmg/u"] = _a(x)
+    out_sol["hpmg/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    r = np.random.default_rng(12).standard_normal(int(fine.Np) * int(fine.K))
+    out_sol["hpmg/vcycle_in"] = r
+    out_sol["hpmg/vcycle_out"] = _a(pc(r))
+    print(f"hpmg {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+
+    for fname, d in (("refelem.npz", out_ref), ("meshes.npz", out_mesh), ("applies.npz", out_app),
+                     ("solves.npz", out_sol)):
+        np.savez_compressed(os.path.join(HERE, fname), **{k: np.asarray(v) for k, v in d.items()})
+    print(f"wrote fixtures in {time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")

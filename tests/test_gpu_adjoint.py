@@ -68,7 +68,7 @@ def test_adjoint_gradient_matches_dense_oracle():
     g_ref = -kap * osp.grad_kappa(o, u.reshape(o.K, o.Np).T, lam.reshape(o.K, o.Np).T, bc_types=bc,
                                   tau_scale=0.5, kappa=kap)
     op = p.device_operator(bc, 0.5)
-    adjoint._state(op).use(np.exp(g_obs))
+    adjoint._state(op).use(op, np.exp(g_obs))
     uo, _ = adjoint._cg(op, adjoint.mass_apply(op, _t(f.T.reshape(-1))), 1e-14, 20000)
     L, G, _ = adjoint.loss_and_grad(op, _t(g[None, :]), _t(f.T.reshape(-1)), uo, tol=1e-14)
     assert np.max(np.abs(G[0].cpu().numpy() - g_ref)) < 1e-8 * np.max(np.abs(g_ref))
@@ -82,7 +82,7 @@ def test_adjoint_gradient_vs_centred_differences():
     o, p, bc, f, g_obs, g = _problem(K=8, N=4, seed=3)
     op = p.device_operator(bc, 0.5)
     ft = _t(f.T.reshape(-1))
-    adjoint._state(op).use(np.exp(g_obs))
+    adjoint._state(op).use(op, np.exp(g_obs))
     uo, _ = adjoint._cg(op, adjoint.mass_apply(op, ft), 1e-14, 40000)
     gt = _t(g)
     _, G, _ = adjoint.loss_and_grad(op, gt[None, :], ft, uo, tol=1e-14, maxiter=40000)

@@ -163,3 +163,52 @@ def test_hpmg_pure_neumann_regularised():
                               iterative=osp.IterativeConfig(tol=1e-12, maxiter=5000))
     assert info.status == "converged" and _rel(u, u_ref) < 1e-7
     assert abs(u.sum()) < 1e-8 * np.abs(u).sum()
+
+
+def test_mesh_cache_eviction_keeps_multigrid_levels_alive():
+    """Filling the mesh's operator cache with other (BC, penalty) pairs drops
+    the cache's reference to a multigrid level operator but must not free the
+    handle the V-cycle still uses; the MG-PCG solve afterwards still matches
+    the direct solve."""
+    import gc
+    from ddg_b200.dg2d import multigrid as pmg
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 3)
+    bc = _dir(o)
+    src = np.random.default_rng(1).standard_normal((o.Np, o.K))
+    mg = pmg.make_sipg_mg_preconditioner(p, bc_types=bc)
+    for tau in (1.0, 2.0, 3.0, 4.0, 5.0):           # five other keys evict the level operator
+        p.device_operator(bc, tau)
+    gc.collect()
+    u, info = _solve_iters(p, bc, src, mg, tol=1e-10)
+    u_lu = ps.solve_sipg_poisson_2d(p, src, bc_types=bc)
+    assert info.status == "converged" and _rel(u, u_lu) < 1e-7
+
+
+def test_operator_destroyed_before_multigrid():
+    """A user operator that captured an MG-CG graph is destroyed before the
+    multigrid object (and the other way round); neither destroy may touch
+    freed memory, and a fresh solve still works."""
+    import torch
+    from ddg_b200.dg2d import multigrid as pmg
+    from ddg_b200.dg2d.operator import SipgOperator
+    o, p = _pair(5, 3)
+    bc = _dir(o)
+    b = torch.as_tensor(np.random.default_rng(2).standard_normal(o.Np * o.K), device="cuda")
+    for order in ("op_first", "mg_first"):
+        mg = pmg.make_sipg_mg_preconditioner(p, bc_types=bc)
+        user = SipgOperator(p, bc, tau_scale=200.0)
+        x = torch.zeros_like(b)
+        st, its, _, _ = user.cg_mg(mg, b, x, tol=1e-10)
+        assert st == "converged"
+        if order == "op_first":
+            user.close()
+            mg.close()
+        else:
+            mg.close()
+            user.close()
+    mg = pmg.make_sipg_mg_preconditioner(p, bc_types=bc)
+    user = SipgOperator(p, bc, tau_scale=200.0)
+    x = torch.zeros_like(b)
+    st, its2, _, _ = user.cg_mg(mg, b, x, tol=1e-10)
+    assert st == "converged" and its2 == its

@@ -486,3 +486,25 @@ def test_fp64_cg_engines_agree(N):
     op.set_engine("tensor")
     assert abs(res["tensor"][0] - res["cuda"][0]) <= 2
     assert np.linalg.norm(res["tensor"][1] - res["cuda"][1]) / np.linalg.norm(res["cuda"][1]) < 1e-9
+
+
+def test_apply_host_follows_engine_switch():
+    """The host-buffer apply recaptures its pipeline after set_engine: results
+    stay equal to the device apply of the engine in force after each switch."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    VX, VY, E = om.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 24, 20)
+    o, p = om.build_mesh_2d(VX, VY, E, 4), pm.build_mesh_2d(VX, VY, E, 4)
+    bc = _bcs(o)["mixed"]
+    from ddg_b200.dg2d.operator import SipgOperator
+    op = SipgOperator(p, bc, tau_scale=0.5)
+    u = np.random.default_rng(5).standard_normal((o.Np, o.K))
+    ref = osp.flat_op(o, bc_types=bc, alpha=5.0, tau_scale=0.5)(u.T.reshape(-1)).reshape(o.K, o.Np).T
+    for engine in ("tensor", "cuda", "tensor", "cuda"):
+        op.set_engine(engine)
+        dev = op.apply(torch.as_tensor(u.T.reshape(-1), device="cuda"), alpha=5.0).cpu().numpy()
+        dev = dev.reshape(o.K, o.Np).T
+        got = op.apply_host(u, alpha=5.0)
+        assert np.array_equal(got, dev), engine
+        assert _rel(got, ref) < APPLY_RTOL64
+    op.close()
