@@ -40,17 +40,17 @@ ALPHA = 5.0
 TAU_SCALE = 0.5
 
 
-def workload_arrays(build_mesh, uniform_mesh):
-    VX, VY, E = uniform_mesh(0.0, 1.0, 0.0, 1.0, KX, KY)
+def workload_arrays(build_mesh, uniform_mesh, kx=KX, ky=KY):
+    VX, VY, E = uniform_mesh(0.0, 1.0, 0.0, 1.0, kx, ky)
     m = build_mesh(VX, VY, E, NDEG)
     isb = m.EToE == np.arange(m.K)[:, None]
     nxf = m.nx.reshape((m.Nfp, 3, m.K), order="F")[0].T
     bc = np.where(isb, np.where(np.abs(nxf) > 0.5, 1, 2), 0).astype(np.int32)
     rng = np.random.default_rng(0)
-    kx = rng.integers(1, 7, size=8)
-    ky = rng.integers(1, 7, size=8)
+    wx = rng.integers(1, 7, size=8)
+    wy = rng.integers(1, 7, size=8)
     amp = rng.standard_normal(8)
-    f = sum(a * np.sin(np.pi * i * m.x) * np.cos(np.pi * j * m.y) for a, i, j in zip(amp, kx, ky))
+    f = sum(a * np.sin(np.pi * i * m.x) * np.cos(np.pi * j * m.y) for a, i, j in zip(amp, wx, wy))
     return m, bc, f
 
 
@@ -59,6 +59,11 @@ def algorithmic_bytes(K, Np, sv, sg):
     scalars per element, 3 packed int32 neighbour words."""
     return K * (2 * Np * sv + 14 * sg + 12)
 
+
+# side of the reduced precision workload whose solves are graded against the
+# oracle's float64 solution (the full size takes minutes on the host cores)
+SMALL = 64
+SMALL_SOLVES: dict = {}
 
 # DRAM bytes of one float64 tensor-core apply launch on this workload, from
 # an ncu capture (56.16 MB read + 1.23 MB written; y stays in L2)
@@ -231,6 +236,16 @@ def run_ours(args, rank, world, local_rank):
                          "refinements": info.refinements, "status": info.status,
                          "rel_err_vs_fp64_tol1e-13": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u))}
         out["speedup_mixed_vs_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+        # the same two solves on the 64 x 64 version of the workload, graded in
+        # the CPU leg against the oracle's float64 block-Jacobi PCG solution
+        ms, bcs, fs = workload_arrays(pm.build_mesh_2d, pm.uniform_rectangle_mesh_2d, SMALL, SMALL)
+        pcs = ps.make_helmholtz_block_jacobi_preconditioner(ms, alpha=ALPHA, nu=1.0, bc_types=bcs,
+                                                            tau_scale=TAU_SCALE)
+        SMALL_SOLVES.clear()
+        for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
+            cfg = ps.IterativeConfig(tol=args.solve_tol, maxiter=20000, precision=prec, inner_tol=args.inner_tol)
+            SMALL_SOLVES[name] = ps.solve_sipg_helmholtz_2d(ms, fs, alpha=ALPHA, nu=1.0, bc_types=bcs,
+                                                            tau_scale=TAU_SCALE, preconditioner=pcs, iterative=cfg)
         out["note"] = ("block-Jacobi PCG, tol %.0e; latency = host wall clock of the public API call "
                        "(numpy in/out); reference solution = float64 device PCG at tol 1e-13" % args.solve_tol)
         solves = out
@@ -261,6 +276,7 @@ def run_ours(args, rank, world, local_rank):
         "solves": solves,
     }
     if not args.skip_workloads:
+        line["plain"] = plain_leg()
         line["hpmg_pressure_poisson"] = hpmg_leg()
         line["serving"] = serving_leg(args.serving_requests)
         line["adjoint"] = adjoint_leg()
@@ -306,37 +322,99 @@ def hpmg_leg():
         out["vcycle_" + prec] = {"iterations": info.iterations, "status": info.status,
                                  "solve_ms": 1e3 * float(np.median(lat)), "setup_s": setup}
         mg.close()
+    # the plain float64 path on the same system: block-Jacobi PCG
+    pcb = ps.make_sipg_block_jacobi_preconditioner(fin, bc_types=nbc(fin), tau_scale=TAU_SCALE)
+    lat = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ub, info = ps.solve_sipg_poisson_2d(fin, src, bc_types=nbc(fin), tau_scale=TAU_SCALE, preconditioner=pcb,
+                                            iterative=ps.IterativeConfig(tol=1e-8, maxiter=50000), return_info=True)
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t0)
+    out["block_jacobi_fp64"] = {"iterations": info.iterations, "status": info.status,
+                                "solve_ms": 1e3 * float(np.min(lat)),
+                                "rel_diff_vs_vcycle_fp64": float(np.linalg.norm(ub - sol["fp64"]) /
+                                                                 np.linalg.norm(sol["fp64"]))}
     out["dofs"] = int(fin.K * fin.Np)
     out["rel_diff_fp32_vs_fp64"] = float(np.linalg.norm(sol["fp32"] - sol["fp64"]) / np.linalg.norm(sol["fp64"]))
     out["note"] = "latency = host wall clock of solve_sipg_poisson_2d (numpy in/out); set-up (host meshes) apart"
     return out
 
 
-def serving_leg(count=256):
-    """Serving workload, bounded sample: `count` seeded requests (n ~ U{8..96}
+def plain_leg():
+    """Plain workload exactly as specified: 12 x 12 quads -> 288 triangles,
+    N = 4 (4,320 DOFs), Dirichlet from u = sin(pi x) sin(pi y), f = 2 pi^2 u,
+    tau_scale = 0.5, unpreconditioned CG to tol 1e-9, through
+    solve_sipg_poisson_2d.  Matvec, iteration count and L2 error are compared
+    with the numbers the reference's own code produced for this workload
+    (tests/golden, generated from the unmodified reference)."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    gold = os.path.join(ROOT, "tests", "golden")
+    ga, gs = np.load(os.path.join(gold, "applies.npz")), np.load(os.path.join(gold, "solves.npz"))
+    VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 12, 12)
+    m = pm.build_mesh_2d(VX, VY, E, 4)
+    bc = np.where(m.EToE == np.arange(m.K)[:, None], ps.BC_DIRICHLET, 0).astype(np.int32)
+    case = "plain12_N4/dirichlet/tau0.5"
+    Au = ps.sipg_apply_2d(m, ga[case + "/u"], bc_types=ga[case + "/bc"], tau_scale=0.5)
+    mv = float(np.max(np.abs(Au - ga[case + "/Au"])) / np.max(np.abs(ga[case + "/Au"])))
+    ue = np.sin(np.pi * m.x) * np.sin(np.pi * m.y)
+    cfg = ps.IterativeConfig(tol=1e-9)
+    lat = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, info = ps.solve_sipg_poisson_2d(m, 2 * np.pi ** 2 * ue, bc_types=bc, u_dir=ue, tau_scale=0.5,
+                                           iterative=cfg, return_info=True)
+        lat.append(time.perf_counter() - t0)
+
+    def l2(d):
+        return float(np.sqrt(np.sum(m.J * d * (m.ref.M @ d))))
+    return {"workload": "12x12 quads -> 288 triangles, N=4, 4320 DOFs, Dirichlet sin(pi x) sin(pi y), "
+                        "tau_scale=0.5, CG tol 1e-9, no preconditioner",
+            "matvec_rel_err_vs_reference": mv, "cg_iterations": info.iterations,
+            "reference_cg_iterations": int(gs["plain/cg_iterations"]), "status": info.status,
+            "l2_err_vs_exact": l2(u - ue), "reference_l2_err_vs_exact": l2(gs["plain/u_cg"] - ue),
+            "rel_err_vs_reference_solution": float(np.linalg.norm(u - gs["plain/u_cg"]) /
+                                                   np.linalg.norm(gs["plain/u_cg"])),
+            "solve_ms": 1e3 * float(np.median(lat[1:]))}
+
+
+def serving_leg(count=4096, loads=(0.5, 0.8)):
+    """Serving workload: the seeded stream of `count` requests (n ~ U{8..96}
     quads per side, N ~ U{2,3,4}, k^2 ~ U[0,10], Dirichlet, 8-mode source,
-    tol 1e-6 or 1e-9), first all at once (saturation throughput), then with
-    Poisson arrivals at 0.7 x that throughput (latency); one-at-a-time
-    float64 solves of the first 24 requests as the baseline."""
+    tol 1e-6 -- run in the float32 pools -- or 1e-9), admitted against a
+    120 GB HBM budget with the tile autotuner on: first all at once
+    (saturation throughput; the autotuner settles its tiles here), then with
+    Poisson arrivals at each fraction of that throughput in `loads`
+    (latency); one-at-a-time float64 solves of the first 24 requests as the
+    baseline."""
     from ddg_b200 import serving
     eng = serving.ServingEngine(degrees=(2, 3, 4), hbm_budget_bytes=120e9, capacity=4_000_000, max_requests=1024,
                                 pairs=4)
     done = eng.run(serving.make_requests(count=count, seed=0), realtime=False)
     burst = serving.summarize(done, eng.elapsed)
-    rate = 0.7 * burst["solves_per_s"]
-    done = eng.run(serving.make_requests(count=count, seed=1, rate=rate), realtime=True)
-    load = serving.summarize(done, eng.elapsed)
+    out = {"requests": count, "saturation": burst, "load_sweep": []}
+    for frac in loads:
+        rate = frac * burst["solves_per_s"]
+        done = eng.run(serving.make_requests(count=count, seed=1, rate=rate), realtime=True)
+        out["load_sweep"].append({"load_fraction": frac, "arrival_rate_per_s": rate,
+                                  **serving.summarize(done, eng.elapsed)})
+    out["autotuner_tiles"] = eng.tuner.table()
     eng.close()
     _, tb = serving.solve_one_at_a_time(serving.make_requests(count=24, seed=0))
-    return {"requests": count, "saturation": burst, "arrival_rate_per_s": rate, "at_load": load,
-            "one_at_a_time_fp64_solves_per_s": 24.0 / tb,
-            "note": "bounded sample of the 4096-request stream; 120 GB admission budget"}
+    out["one_at_a_time_fp64_solves_per_s"] = 24.0 / tb
+    out["note"] = ("the full 4096-request stream; tol 1e-6 requests iterate in float32 pools, 1e-9 in float64; "
+                   "120 GB admission budget; latency = arrival to retirement on the host clock")
+    return out
 
 
-def adjoint_leg(batch=8, fd_dirs=2):
-    """Differentiation workload, bounded sample: 64 x 64 quads -> 8192
-    triangles, N = 4, kappa = exp(g), g ~ N(0, 0.5^2) per element; gradient of
-    1/2 ||u - u_obs||_M^2 for `batch` of the 64 kappas via the adjoint
+def adjoint_leg(batch=64, fd_dirs=32):
+    """Differentiation workload: 64 x 64 quads -> 8192 triangles, N = 4,
+    kappa = exp(g), g ~ N(0, 0.5^2) per element; gradient of
+    1/2 ||u - u_obs||_M^2 for a batch of `batch` kappas via the adjoint
     (forward + adjoint block-Jacobi PCG + contraction kernel), checked against
     centred differences (h = 1e-6) on `fd_dirs` random directions."""
     import torch
@@ -348,7 +426,7 @@ def adjoint_leg(batch=8, fd_dirs=2):
     op = m.device_operator(bc, TAU_SCALE)
     f = torch.as_tensor((np.sin(np.pi * m.x) * np.sin(np.pi * m.y) + 0.5).T.reshape(-1).copy(), device="cuda")
     g_obs = torch.as_tensor(0.5 * np.random.default_rng(1).standard_normal(m.K), device="cuda")
-    adjoint._state(op).use(torch.exp(g_obs).cpu().numpy())
+    adjoint._state(op).use(op, torch.exp(g_obs).cpu().numpy())
     uo, _ = adjoint._cg(op, adjoint.mass_apply(op, f), 1e-12, 40000)
     G = torch.as_tensor(0.5 * np.random.default_rng(2).standard_normal((batch, m.K)), device="cuda")
     torch.cuda.synchronize()
@@ -367,7 +445,26 @@ def adjoint_leg(batch=8, fd_dirs=2):
         worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-300))
     return {"batch": batch, "gradients_per_s": batch / dt, "cg_iterations": int(its),
             "fd_max_rel_err": worst, "fd_directions": fd_dirs,
-            "note": "bounded sample of the 64-kappa batch; FD h = 1e-6 in float64"}
+            "note": "the 64-kappa batch; centred FD (h = 1e-6, float64) on the first kappa's gradient; "
+                    "the reference has no per-element diffusivity (and JAX is absent), so there is no "
+                    "reference jax.grad to compare with"}
+
+
+def profile_apply(args):
+    """Stand-alone applies of the workload (no L2 flush), for a profiler's
+    capture of one kernel: `--profile-apply fp64` runs the float64 apply,
+    `fp32` the float32 one, each `--profile-reps` times."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    m, bc, _ = workload_arrays(pm.build_mesh_2d, pm.uniform_rectangle_mesh_2d)
+    op = m.device_operator(bc, TAU_SCALE)
+    dt = torch.float64 if args.profile_apply == "fp64" else torch.float32
+    u = torch.randn(op.n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1)).to(dt)
+    y = torch.empty_like(u)
+    for _ in range(args.profile_reps):
+        op.apply(u, alpha=ALPHA, out=y)
+    torch.cuda.synchronize()
+    print(f"{args.profile_reps} {args.profile_apply} applies done", flush=True)
 
 
 def profile_solves(args):
@@ -390,9 +487,31 @@ def profile_solves(args):
 # ------------------------------------------------------------ CPU legs
 
 def cpu_baseline(budget_s=15.0):
-    """The oracle's float64 apply on the host cores, bounded sample."""
+    """The oracle's float64 apply on the host cores, bounded sample; then the
+    oracle's float64 block-Jacobi PCG solve (C + OpenMP apply, numpy block
+    inverses, the reference's CG stopping rule) of the 64 x 64 version of the
+    workload, timed, and the GPU solutions of the same system graded
+    against it."""
     from oracle import cbuild
-    return cbuild.time_apply(KX, KY, NDEG, TAU_SCALE, ALPHA, budget_s=budget_s)
+    from oracle import mesh as om
+    from oracle import sipg as osp
+    out = cbuild.time_apply(KX, KY, NDEG, TAU_SCALE, ALPHA, budget_s=budget_s)
+    m, bc, f = workload_arrays(om.build_mesh_2d, om.uniform_rectangle_mesh_2d, SMALL, SMALL)
+    A = cbuild.CApply(m, bc, TAU_SCALE, ALPHA)
+    t0 = time.perf_counter()
+    pc = osp.block_jacobi_from_blocks(osp.extract_block_diag_matfree(A, m))
+    b = osp._rhs(m, f, bc, None, None, TAU_SCALE)
+    x, its = osp.cg(A, b, tol=1e-10, maxiter=20000, M=pc)
+    dt = time.perf_counter() - t0
+    u = x.reshape(m.K, m.Np).T
+    solve = {"workload": f"{SMALL}x{SMALL} quads -> {2 * SMALL * SMALL} triangles, N={NDEG}, {m.K * m.Np} DOFs, "
+                         "same BCs, alpha, tau_scale and RHS as the full workload",
+             "oracle_block_jacobi_pcg": {"iterations": int(its), "solve_s": dt, "tol": 1e-10,
+                                         "cores": len(os.sched_getaffinity(0))}}
+    for name, ug in SMALL_SOLVES.items():
+        solve[f"rel_l2_err_{name}_vs_oracle"] = float(np.linalg.norm(ug - u) / np.linalg.norm(u))
+    out["solve"] = solve
+    return out
 
 
 def run_reference(args, rank, world):
@@ -400,13 +519,14 @@ def run_reference(args, rank, world):
         return None
     from oracle import cbuild
     step, ndof, nt = cbuild.apply_stepper(KX, KY, NDEG, TAU_SCALE, ALPHA)
-    for _ in range(args.warmup):
+    per = max(1, -(-50 // max(1, args.steps)))      # at least 50 timed applies in all
+    for _ in range(args.warmup * per):
         step()
-    ts = [step() for _ in range(args.steps)]
+    ts = [step() for _ in range(args.steps * per)]
     t = float(np.median(ts))
     v = ndof / t / 1e9
     cb = {"value": v, "unit": "GDOF/s", "cores": nt, "kind": "port",
-          "sample": f"{args.steps} timed float64 applies (one per step, after {args.warmup} warm-up applies) of the "
+          "sample": f"{len(ts)} timed float64 applies ({per} per step, after {args.warmup * per} warm-up applies) of the "
                     f"full {2 * KX * KY}-element N={NDEG} mesh; C+OpenMP restatement of the reference operator; "
                     f"median {t * 1e3:.2f} ms",
           "median_ms": t * 1e3}
@@ -434,17 +554,23 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-workloads", action="store_true",
                     help="leave out the multigrid, serving and adjoint legs")
-    ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-requests", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile-maxiter", type=int, default=20000)
     ap.add_argument("--profile-solves", action="store_true",
                     help="only the float64 and mixed solves, one each (for a profiler's launch list)")
+    ap.add_argument("--profile-apply", choices=["fp64", "fp32"], default=None,
+                    help="only stand-alone applies of one precision (for a profiler's capture of that kernel)")
+    ap.add_argument("--profile-reps", type=int, default=5)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.profile_solves:
         profile_solves(args)
+        return
+    if args.profile_apply:
+        profile_apply(args)
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)

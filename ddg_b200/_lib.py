@@ -83,10 +83,13 @@ _PROTOS = {
     "ddg_mg_apply": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ddg_sipg_cg_mg": (C.c_int, [_vp, C.POINTER(CgConfig), _vp, _vp, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_pool_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(_vp)]),
+    "ddg_pool_create_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                     C.POINTER(_vp)]),
     "ddg_pool_destroy": (C.c_int, [_vp]),
     "ddg_pool_admit": (C.c_int, [_vp, C.POINTER(MeshDesc), C.c_double, C.c_double, C.c_double, C.c_int, _vp, _vp,
                                  C.POINTER(C.c_int)]),
     "ddg_pool_iterate": (C.c_int, [_vp, C.c_int, _vp]),
+    "ddg_pool_set_tile": (C.c_int, [_vp, C.c_int, C.c_int]),
     "ddg_pool_poll": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ddg_pool_retire": (C.c_int, [_vp, C.c_int, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_sipg_upload_reference": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, C.c_int]),

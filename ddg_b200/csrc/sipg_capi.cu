@@ -146,7 +146,7 @@ struct ddg_sipg_op {
   HostIO* hio = nullptr;            // host-buffer apply state (lazy)
   uint8_t* tc_img = nullptr;        // tensor-core B operands of this degree (device)
   int fp32_engine = DDG_ENGINE_TENSOR_CORES;   // stand-alone float32 applies
-  int cg32_engine = DDG_ENGINE_CUDA_CORES;     // float32 CG iterations (fewer iterations in mixed solves)
+  int cg32_engine = DDG_ENGINE_TENSOR_CORES;   // float32 CG iterations (CUDA cores where no tensor-core apply is built)
   double* dm_img = nullptr;         // FP64 tensor-core (DMMA) B operands of this degree (device)
   double* dm_geo = nullptr;         // that kernel's element and face coefficients (device)
   int fp64_engine = DDG_ENGINE_TENSOR_CORES;   // every float64 apply (stand-alone, CG, residuals)
@@ -293,10 +293,21 @@ int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGra
     a.out0 = (T*)w.Ap;
     a.out1 = (T*)pout;
     if constexpr (sizeof(T) == 4) {
-      if (key.engine == DDG_ENGINE_TENSOR_CORES)
-        e = launch_apply_tc(op->N, AM_PFUSE, a, op->tc_img, op->cap);
-      else
+      if (key.engine == DDG_ENGINE_TENSOR_CORES) {
+        // the direction first (one streaming pass), then the tensor-core
+        // apply of the formed direction with the p.Ap reduction: its
+        // neighbour gathers read one vector instead of two
+        e = launch_pupd((int64_t)op->K * op->Np, (const float*)c.z, (const float*)pin, (float*)pout, op->ctl,
+                        op->cap);
+        if (e == cudaSuccess) {
+          a.in0 = (const T*)pout;
+          a.in1 = nullptr;
+          a.out1 = nullptr;
+          e = launch_apply_tc(op->N, AM_PDOT, a, op->tc_img, op->cap);
+        }
+      } else {
         e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+      }
     } else {
       e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
     }
@@ -528,7 +539,7 @@ extern "C" int ddg_sipg_create(const ddg_sipg_mesh_desc* d, ddg_sipg_op** out) {
     if (e == cudaSuccess) e = cudaMemcpy(op->tc_img, img.data(), img.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = tc_prepare(N);
   }
-  if (!tc_supported(N)) op->fp32_engine = DDG_ENGINE_CUDA_CORES;
+  if (!op->tc_img) op->fp32_engine = op->cg32_engine = DDG_ENGINE_CUDA_CORES;
   if (e == cudaSuccess && dm_supported(N)) {
     std::vector<double> img((size_t)dm_image_doubles(N), 0.0);
     dm_build_image(N, d->Dr, d->Ds, d->M, d->m1d, img.data());

@@ -1238,6 +1238,33 @@ cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, doubl
   k_axpby<<<vec_grid(n), 256, 0, s>>>(n, al, x, be, y);
   return cudaGetLastError();
 }
+// p = zc z + beta p_old for the CG direction (zc, beta from the control
+// block; nothing once the loop has stopped), float32, four values per thread
+// step; the same rounding as the fused direction update of the applies
+__global__ void k_pupd(int64_t n, const float* __restrict__ z, const float* __restrict__ p_old,
+                       float* __restrict__ p, const CgCtl* ctl) {
+  if (ctl->cont == 0) return;
+  const float zc = (float)ctl->zcoef, be = (float)ctl->beta;
+  const int64_t n4 = n / 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const float4 a = reinterpret_cast<const float4*>(z)[i];
+    const float4 b = reinterpret_cast<const float4*>(p_old)[i];
+    float4 c;
+    c.x = fmaf(zc, a.x, be * b.x);
+    c.y = fmaf(zc, a.y, be * b.y);
+    c.z = fmaf(zc, a.z, be * b.z);
+    c.w = fmaf(zc, a.w, be * b.w);
+    reinterpret_cast<float4*>(p)[i] = c;
+  }
+  for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    p[i] = fmaf(zc, z[i], be * p_old[i]);
+}
+cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s) {
+  k_pupd<<<vec_grid((n + 3) / 4), 256, 0, s>>>(n, z, p_old, p, ctl);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s) {
   if (to_prec == 1) k_cast<double, float><<<vec_grid(n), 256, 0, s>>>(n, (const double*)src, (float*)dst);
   else k_cast<float, double><<<vec_grid(n), 256, 0, s>>>(n, (const float*)src, (double*)dst);

@@ -8,7 +8,9 @@ namespace ddg {
 
 struct CgCtl;
 
-enum ApplyMode { AM_APPLY = 0, AM_PFUSE = 1, AM_RESID = 2, AM_SMOOTH = 3 };
+// AM_PDOT (tensor-core float32 apply only): y = A p for an already formed
+// direction p, with the p.Ap reduction and alpha of AM_PFUSE.
+enum ApplyMode { AM_APPLY = 0, AM_PFUSE = 1, AM_RESID = 2, AM_SMOOTH = 3, AM_PDOT = 4 };
 
 template <typename T>
 struct ApplyArgs {
@@ -105,6 +107,12 @@ struct BatchArgs {
   const int* perm;
   double tau;
   int max_req;
+  int threads;             // element-kernel tile: threads per block (64, 128 or 256)
+  int persistent;          // 1: a persistent grid of a few blocks per SM
+  int prec;                // iteration vectors: 0 float64 (x, r, z, Ap above), 1 float32 (below)
+  const float* geo32;      // float32 copies of geo and binv (float32 pools)
+  const float* binv32;
+  float *x32, *r32, *z32, *Ap32;
 };
 
 struct RhsArgs {
@@ -160,6 +168,8 @@ cudaError_t launch_rhs(int N, const RhsArgs& a, cudaStream_t s);
 cudaError_t launch_grad_kappa(int N, const GradArgs& a, cudaStream_t s);
 cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, double* y, cudaStream_t s);
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s);
+// float32 CG direction p = zc z + beta p_old (16-byte aligned vectors)
+cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s);
 // r32 = float(r64), x32 = 0, ctl->bb = r32.r32 (reliable-update restart)
 cudaError_t launch_cast_norm(int64_t n, const double* r64, float* r32, float* x32, double* part, CgCtl* ctl,
                              cudaStream_t s);
@@ -181,10 +191,13 @@ cudaError_t launch_cg_finish(bool init, const T* r, const T* z, int64_t n, CgCtl
                              const unsigned int* dev_status, int has_cond, cudaGraphConditionalHandle cond,
                              cudaStream_t s);
 int xr_grid(int64_t n);
-cudaError_t launch_batch_pfuse(int N, const BatchArgs& a, const double* pin, double* pout, cudaStream_t s);
-cudaError_t launch_batch_step(int N, const BatchArgs& a, const double* p, cudaStream_t s);
+// pin / pout / p / p0: float64 or float32 vectors as a.prec says
+cudaError_t launch_batch_pfuse(int N, const BatchArgs& a, const void* pin, void* pout, cudaStream_t s);
+cudaError_t launch_batch_step(int N, const BatchArgs& a, const void* p, cudaStream_t s);
 cudaError_t launch_batch_seg(int mode, const BatchArgs& a, int first_req, int nreq, cudaStream_t s);
-cudaError_t launch_batch_init(int N, const BatchArgs& a, double* p0, int k0, int K, cudaStream_t s);
+cudaError_t launch_batch_init(int N, const BatchArgs& a, void* p0, int k0, int K, cudaStream_t s);
+// float32 copy of `rows` SoA rows of elements [k0, k0 + K) (row stride ld)
+cudaError_t launch_rows_to_f32(const double* src, float* dst, int rows, int ld, int k0, int K, cudaStream_t s);
 cudaError_t launch_batch_rhs(int N, const BatchArgs& a, const double* f, int k0, int K, cudaStream_t s);
 // host: neighbour words of a mesh, element ids shifted by k_offset
 int pack_neighbours(int K, int N, const int64_t* EToE, const int64_t* EToF, const int64_t* vmapP,

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <array>
 #include <map>
 #include <string>
 #include <vector>
@@ -36,7 +37,12 @@ struct ddg_pool {
   int* seg = nullptr;
   double* alpha_e = nullptr;
   double* binv = nullptr;
-  double *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *Ap = nullptr;
+  int prec = DDG_FP64;          // iteration vectors: DDG_FP64 or DDG_FP32
+  double *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *Ap = nullptr;   // float64 pools
+  float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *Ap32 = nullptr;          // float32 pools
+  void *p0 = nullptr, *p1 = nullptr;      // CG directions (the pool's precision)
+  float *geo32 = nullptr, *binv32 = nullptr;  // float32 copies (float32 pools)
+  double* fsrc = nullptr;       // admission scratch: the request's source (max request size)
   double *epA = nullptr, *epB = nullptr;
   BatchReq* req = nullptr;
   int* perm = nullptr;
@@ -46,7 +52,9 @@ struct ddg_pool {
   // host
   std::vector<std::pair<int, int>> free_ranges;   // (start, length), sorted by start
   std::vector<int> slot_k0, slot_K;               // -1 when the slot is free
-  std::map<std::pair<int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;  // (hw, pairs)
+  int threads = 128, persistent = 0;              // element-kernel tile (ddg_pool_set_tile)
+  // captured iteration graphs by (hw, pairs, threads, persistent)
+  std::map<std::array<int, 4>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
   cudaStream_t cap_stream = nullptr;
 };
 
@@ -57,6 +65,8 @@ namespace {
 
 BatchArgs pool_args(ddg_pool* p) {
   BatchArgs a{};
+  a.threads = p->threads;
+  a.persistent = p->persistent;
   a.cap = p->cap;
   a.hw = p->hw;
   a.geo = p->geo;
@@ -69,6 +79,13 @@ BatchArgs pool_args(ddg_pool* p) {
   a.r = p->r;
   a.z = p->z;
   a.Ap = p->Ap;
+  a.prec = p->prec == DDG_FP32 ? 1 : 0;
+  a.geo32 = p->geo32;
+  a.binv32 = p->binv32;
+  a.x32 = p->x32;
+  a.r32 = p->r32;
+  a.z32 = p->z32;
+  a.Ap32 = p->Ap32;
   a.epA = p->epA;
   a.epB = p->epB;
   a.req = p->req;
@@ -84,7 +101,8 @@ void pool_free(ddg_pool* p) {
     cudaGraphDestroy(kv.second.first);
   }
   void* d[] = {p->geo, p->nbr, p->seg, p->alpha_e, p->binv, p->x, p->b, p->r, p->z, p->p0, p->p1, p->Ap,
-               p->epA, p->epB, p->req, p->perm, p->blocks, p->status};
+               p->epA, p->epB, p->req, p->perm, p->blocks, p->status, p->x32, p->r32, p->z32, p->Ap32,
+               p->geo32, p->binv32, p->fsrc};
   for (void* q : d)
     if (q) cudaFree(q);
   if (p->req_host) cudaFreeHost(p->req_host);
@@ -119,7 +137,7 @@ void give_range(ddg_pool* p, int k0, int K) {
 }
 
 int pool_graph(ddg_pool* p, int pairs, cudaGraphExec_t* out) {
-  auto key = std::make_pair(p->hw, pairs);
+  const std::array<int, 4> key{p->hw, pairs, p->threads, p->persistent};
   auto it = p->graphs.find(key);
   if (it != p->graphs.end()) {
     *out = it->second.second;
@@ -129,8 +147,8 @@ int pool_graph(ddg_pool* p, int pairs, cudaGraphExec_t* out) {
   PCK(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int it2 = 0; it2 < 2 * pairs && e == cudaSuccess; ++it2) {
-    double* pin = (it2 % 2 == 0) ? p->p0 : p->p1;
-    double* pout = (it2 % 2 == 0) ? p->p1 : p->p0;
+    void* pin = (it2 % 2 == 0) ? p->p0 : p->p1;
+    void* pout = (it2 % 2 == 0) ? p->p1 : p->p0;
     e = launch_batch_pfuse(p->N, a, pin, pout, p->cap_stream);
     if (e == cudaSuccess) e = launch_batch_seg(0, a, 0, p->max_req, p->cap_stream);
     if (e == cudaSuccess) e = launch_batch_step(p->N, a, pout, p->cap_stream);
@@ -153,8 +171,14 @@ int pool_graph(ddg_pool* p, int pairs, cudaGraphExec_t* out) {
 
 extern "C" int ddg_pool_create(int N, int capacity, int max_requests, int max_request_K, double tau_scale,
                                int device, ddg_pool** out) {
+  return ddg_pool_create_ex(N, capacity, max_requests, max_request_K, tau_scale, DDG_FP64, device, out);
+}
+
+extern "C" int ddg_pool_create_ex(int N, int capacity, int max_requests, int max_request_K, double tau_scale,
+                                  int precision, int device, ddg_pool** out) {
   if (!out || N < 1 || N > DDG_MAX_DEGREE || capacity < 1 || (uint32_t)capacity > NBR_MAX_K ||
-      max_requests < 1 || max_request_K < 1 || max_request_K > capacity)
+      max_requests < 1 || max_request_K < 1 || max_request_K > capacity ||
+      (precision != DDG_FP64 && precision != DDG_FP32))
     return fail(DDG_ERR_INVALID, "ddg_pool_create: bad arguments");
   *out = nullptr;
   int cur = 0;
@@ -177,13 +201,26 @@ extern "C" int ddg_pool_create(int N, int capacity, int max_requests, int max_re
   PA(p->seg, nE * 4);
   PA(p->alpha_e, nE * 8);
   PA(p->binv, nS * nE * 8);
-  PA(p->x, nV * 8);
   PA(p->b, nV * 8);
-  PA(p->r, nV * 8);
-  PA(p->z, nV * 8);
-  PA(p->p0, nV * 8);
-  PA(p->p1, nV * 8);
-  PA(p->Ap, nV * 8);
+  PA(p->fsrc, (size_t)max_request_K * p->Np * 8);
+  p->prec = precision;
+  if (precision == DDG_FP64) {
+    PA(p->x, nV * 8);
+    PA(p->r, nV * 8);
+    PA(p->z, nV * 8);
+    PA(p->p0, nV * 8);
+    PA(p->p1, nV * 8);
+    PA(p->Ap, nV * 8);
+  } else {
+    PA(p->x32, nV * 4);
+    PA(p->r32, nV * 4);
+    PA(p->z32, nV * 4);
+    PA(p->p0, nV * 4);
+    PA(p->p1, nV * 4);
+    PA(p->Ap32, nV * 4);
+    PA(p->geo32, G_COUNT * nE * 4);
+    PA(p->binv32, nS * nE * 4);
+  }
   PA(p->epA, nE * 8);
   PA(p->epB, nE * 8);
   PA(p->req, max_requests * sizeof(BatchReq));
@@ -271,9 +308,8 @@ extern "C" int ddg_pool_admit(ddg_pool* p, const ddg_sipg_mesh_desc* d, double a
                           cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(p->perm, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(p->alpha_e + k0, alv.data(), (size_t)K * 8, cudaMemcpyHostToDevice, st);
-  // source into r (scratch), b = J M f
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(p->r + (size_t)k0 * Np, f, (size_t)K * Np * 8, cudaMemcpyHostToDevice, st);
+  // source into the scratch, b = J M f
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p->fsrc, f, (size_t)K * Np * 8, cudaMemcpyHostToDevice, st);
   // block-Jacobi blocks of the range
   BlockArgs ba{};
   ba.geo = p->geo;
@@ -291,7 +327,11 @@ extern "C" int ddg_pool_admit(ddg_pool* p, const ddg_sipg_mesh_desc* d, double a
   ba.nbr_ld = p->cap;
   if (e == cudaSuccess) e = launch_block_jacobi(p->N, ba, st);
   BatchArgs a = pool_args(p);
-  if (e == cudaSuccess) e = launch_batch_rhs(p->N, a, p->r + (size_t)k0 * Np, k0, K, st);
+  if (e == cudaSuccess && p->prec == DDG_FP32) {   // float32 copies of the range's geometry and inverses
+    e = launch_rows_to_f32(p->geo, p->geo32, G_COUNT, p->cap, k0, K, st);
+    if (e == cudaSuccess) e = launch_rows_to_f32(p->binv, p->binv32, Np * (Np + 1) / 2, p->cap, k0, K, st);
+  }
+  if (e == cudaSuccess) e = launch_batch_rhs(p->N, a, p->fsrc, k0, K, st);
   if (e == cudaSuccess) e = launch_batch_init(p->N, a, p->p0, k0, K, st);
   BatchReq q{};
   q.k0 = k0;
@@ -330,6 +370,18 @@ extern "C" int ddg_pool_iterate(ddg_pool* p, int pairs, void* stream) {
   return rc;
 }
 
+// Tile shape of the element kernels of later ddg_pool_iterate calls:
+// threads per block (64, 128 or 256) and persistent (0: one thread per
+// element; 1: at most 2048 / threads blocks per SM looping over the
+// elements).  Results do not depend on it.
+extern "C" int ddg_pool_set_tile(ddg_pool* p, int threads, int persistent) {
+  if (!p || !(threads == 64 || threads == 128 || threads == 256) || (persistent != 0 && persistent != 1))
+    return fail(DDG_ERR_INVALID, "ddg_pool_set_tile: threads must be 64, 128 or 256 and persistent 0 or 1");
+  p->threads = threads;
+  p->persistent = persistent;
+  return DDG_OK;
+}
+
 // Copy the per-request state to the host and report, per slot, 1 when the
 // request is still iterating, 0 when it has finished (or the slot is empty).
 extern "C" int ddg_pool_poll(ddg_pool* p, int32_t* active, int32_t* iterations, void* stream) {
@@ -361,13 +413,22 @@ extern "C" int ddg_pool_retire(ddg_pool* p, int slot, double* x, void* stream, d
     cudaSetDevice(cur);
     return fail(DDG_ERR_INVALID, "ddg_pool_retire: request still iterating");
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(x, p->x + (size_t)k0 * p->Np, (size_t)K * p->Np * 8, cudaMemcpyDeviceToHost, st);
+  std::vector<float> x32;
+  if (e == cudaSuccess) {
+    if (p->prec == DDG_FP64) {
+      e = cudaMemcpyAsync(x, p->x + (size_t)k0 * p->Np, (size_t)K * p->Np * 8, cudaMemcpyDeviceToHost, st);
+    } else {
+      x32.resize((size_t)K * p->Np);
+      e = cudaMemcpyAsync(x32.data(), p->x32 + (size_t)k0 * p->Np, x32.size() * 4, cudaMemcpyDeviceToHost, st);
+    }
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(p->seg + k0, 0xff, (size_t)K * 4, st);
   BatchReq zero{};
   if (e == cudaSuccess) e = cudaMemcpyAsync(p->req + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cudaSetDevice(cur);
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("ddg_pool_retire: ") + cudaGetErrorString(e));
+  for (size_t i = 0; i < x32.size(); ++i) x[i] = (double)x32[i];
   p->slot_k0[slot] = -1;
   p->slot_K[slot] = 0;
   give_range(p, k0, K);

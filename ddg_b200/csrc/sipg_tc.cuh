@@ -132,11 +132,16 @@ __device__ __forceinline__ uint32_t tf32_bits(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
 }
-// x = hi + lo, both representable in TF32
+// x = hi + lo, both TF32: hi is x rounded to TF32 (nearest, ties away from
+// zero: add half a unit of the 10-bit mantissa to the magnitude bits and
+// clear the 13 low bits -- a carry into the exponent is the correct
+// rounding; finite inputs only), lo the TF32 rounding of the exact float32
+// remainder x - hi.
 __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = tf32_bits(x);
+  hi = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
   lo = tf32_bits(x - __uint_as_float(hi));
 }
+
 
 // shared-memory matrix descriptor, K-major, no swizzle
 __device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo, uint32_t sbo) {
@@ -217,21 +222,25 @@ __device__ __forceinline__ void store_split(uint32_t taddr_lane, int col, const 
 //   p = zc z + beta p_old (beta, zc from the control block), p_new = p,
 //   y = A p, and the last CTA to finish turns the per-CTA partials of p.Ap
 //   into ctl->pAp and ctl->alpha = gamma / pAp (breakdown flagged).
+// MODE AM_PDOT: the same with p already formed (u = p): one input tile and
+//   plain neighbour gathers.
 template <int N, int MODE>
 __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs a) {
   using D = TcDim<N>;
   constexpr int Np = D::Np, Nfp = D::Nfp, Kp = D::Kp, K2 = D::K2;
   constexpr int NT = (MODE == AM_PFUSE) ? 2 : 1;  // input tiles per element tile
+  constexpr bool DOT = (MODE == AM_PFUSE || MODE == AM_PDOT);  // p.Ap and alpha
   constexpr int TILE = 128 * Np;                   // floats per tile
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* s_img = smem;                                          // IMG_BYTES
   float* s_t = reinterpret_cast<float*>(smem + D::IMG_BYTES);     // [2 buffers][NT][TILE]
   int* s_perm = reinterpret_cast<int*>(s_t + 2 * NT * TILE);      // 3 Np
   __shared__ __align__(8) uint64_t bar_img, bar_u[2], bar_mma;
+  __shared__ float s_msum[Np];                                    // row sums of M (centring)
   __shared__ uint32_t s_taddr;
   __shared__ double s_red[64];
 
-  if (MODE == AM_PFUSE && a.ctl->cont == 0) return;  // the loop has stopped (uniform)
+  if (DOT && a.ctl->cont == 0) return;  // the loop has stopped (uniform)
   const RefMats<N, float>& R = CRef<N, float>::get();
   const RefPairs<N>& P = CPairs<N>::get();
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -251,6 +260,11 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
     fence_mbar_init();
   }
   for (int i = tid; i < 3 * Np; i += 128) s_perm[i] = a.perm[i];
+  if (tid < Np) {
+    float m = 0.0f;
+    for (int j = 0; j < Np; ++j) m += R.M[tid * Np + j];
+    s_msum[tid] = m;
+  }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -324,8 +338,20 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
       if (a.kappa) kM = __ldg(a.kappa + k);
     }
 
-    // ---- stage 1: A = u (3xTF32) into TMEM, MMA into D1
-    store_split<Kp>(tlane, D::COL_AU, u, Np);
+    // ---- stage 1: A = u - c (3xTF32) into TMEM, MMA into D1.  The
+    // stiffness and derivative blocks annihilate constants, so centring on
+    // c = u[0] leaves them unchanged while their float32 rounding error
+    // scales with the element's variation instead of |u| (the mass block
+    // gets c M 1 back in the epilogue); on smooth vectors, the slow modes of
+    // an iterative solve, this removes a cancellation error of order
+    // eps / (k h)^2.
+    const float c0 = u[0];
+    {
+      float uc[Np];
+#pragma unroll
+      for (int i = 0; i < Np; ++i) uc[i] = u[i] - c0;
+      store_split<Kp>(tlane, D::COL_AU, uc, Np);
+    }
     tmem_wait_st();
     fence_before_sync();
     __syncthreads();
@@ -370,7 +396,10 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
         for (int q = 0; q < Nfp; ++q) {
           float2 s = make_float2(0.0f, 0.0f);  // (Dr_F0 u~, Ds_F0 u~), packed FP32 FMA
 #pragma unroll
-          for (int j = 0; j < Np; ++j) s = __ffma2_rn(P.DrDs[q * Np + j], make_float2(ut[j], ut[j]), s);
+          for (int j = 0; j < Np; ++j) {
+            const float v = ut[j] - c0;  // centred as the own values
+            s = __ffma2_rn(P.DrDs[q * Np + j], make_float2(v, v), s);
+          }
           dq[q] = cr * s.x + cs * s.y;
         }
 #pragma unroll
@@ -409,7 +438,7 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
               if (blk == 0) y[n] = fmaf(crr, v[i], y[n]);
               else if (blk == 1) y[n] = fmaf(crs, v[i], y[n]);
               else if (blk == 2) y[n] = fmaf(css, v[i], y[n]);
-              else if (blk == 3) y[n] = fmaf(cm, v[i], y[n]);
+              else if (blk == 3) y[n] = fmaf(cm, v[i] + c0 * s_msum[n], y[n]);
               else if (blk == 4) dr[n] = v[i];
               else ds[n] = v[i];
             }
@@ -501,7 +530,7 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
 #pragma unroll
       for (int i = 0; i < Np; ++i) y[i] = fmaf(a.shift, u[i], y[i]);
     }
-    if (MODE == AM_PFUSE && active) {
+    if (DOT && active) {
 #pragma unroll
       for (int i = 0; i < Np; ++i) dA += (double)u[i] * (double)y[i];
     }
@@ -542,7 +571,7 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
   fence_before_sync();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tbase, D::TMEM_COLS);
-  if (MODE != AM_PFUSE) return;
+  if (!DOT) return;
 
   // ---- p.Ap: CTA partial -> last CTA -> control block (every CTA takes part,
   // also after a time-out, so the ticket always completes)
@@ -636,6 +665,7 @@ int build_image(const double* Dr, const double* Ds, const double* M, uint8_t* ou
 // Degrees with a tensor-core float32 apply.
 bool tc_supported(int N) { return N >= 1 && N <= 4; }
 
+
 int tc_image_bytes(int N) {
   switch (N) {
     case 1: return tc::TcDim<1>::IMG_BYTES;
@@ -682,6 +712,13 @@ cudaError_t tc_prepare(int N) {
     case 2: e = tc_prepare_n<2, AM_APPLY>(); if (e == cudaSuccess) e = tc_prepare_n<2, AM_PFUSE>(); break;
     case 3: e = tc_prepare_n<3, AM_APPLY>(); if (e == cudaSuccess) e = tc_prepare_n<3, AM_PFUSE>(); break;
     case 4: e = tc_prepare_n<4, AM_APPLY>(); if (e == cudaSuccess) e = tc_prepare_n<4, AM_PFUSE>(); break;
+  }
+  if (e != cudaSuccess) return e;
+  switch (N) {
+    case 1: e = tc_prepare_n<1, AM_PDOT>(); break;
+    case 2: e = tc_prepare_n<2, AM_PDOT>(); break;
+    case 3: e = tc_prepare_n<3, AM_PDOT>(); break;
+    case 4: e = tc_prepare_n<4, AM_PDOT>(); break;
   }
   return e;
 }
@@ -730,6 +767,7 @@ static cudaError_t launch_tc_mode(int N, const ApplyArgs<float>& a, const uint8_
 cudaError_t launch_apply_tc(int N, int mode, const ApplyArgs<float>& a, const uint8_t* img, cudaStream_t s) {
   if (mode == AM_APPLY) return launch_tc_mode<AM_APPLY>(N, a, img, s);
   if (mode == AM_PFUSE) return launch_tc_mode<AM_PFUSE>(N, a, img, s);
+  if (mode == AM_PDOT) return launch_tc_mode<AM_PDOT>(N, a, img, s);
   return cudaErrorInvalidValue;
 }
 

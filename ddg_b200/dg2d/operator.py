@@ -131,9 +131,8 @@ class SipgOperator:
     def set_engine(self, engine: str):
         """Apply engine: "tensor" (float32 on tcgen05 with 3xTF32 splitting,
         degrees 1..4; float64 on the FP64 tensor cores, mma.sync f64, degrees
-        1..5) or "cuda" (plain FMA on the CUDA cores).  Defaults: tensor cores
-        for every float64 apply and stand-alone float32 applies, CUDA cores
-        for float32 CG iterations."""
+        1..5) or "cuda" (plain FMA on the CUDA cores).  Default: tensor cores
+        for every apply (float64, float32, and the float32 CG iterations)."""
         code = {"tensor": _lib.DDG_ENGINE_TENSOR_CORES, "cuda": _lib.DDG_ENGINE_CUDA_CORES}[engine]
         _lib.check(_lib.lib().ddg_sipg_set_engine(self._h, code), "ddg_sipg_set_engine")
 

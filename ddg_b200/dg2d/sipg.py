@@ -47,6 +47,12 @@ class IterativeConfig:
     inner_tol: float = 0.7       # mixed: float32 residual reduction between float64 updates
     max_refinements: int = 50    # mixed-restart: outer iteration cap
     restart: int = 30            # gmres
+    # pure-Neumann (singular) Poisson: "shift" is the reference's epsilon
+    # shift (sipg.py:891-906); "project" solves the consistent singular system
+    # exactly (RHS projected onto range(A) = 1-perp, no shift) and returns the
+    # solution with zero mean over the DOFs -- the limit the shifted solution
+    # approaches as epsilon -> 0
+    nullspace: str = "shift"
 
 
 @dataclass
@@ -419,16 +425,22 @@ def solve_sipg_poisson_2d(mesh: Mesh2D, source, *, bc_types, u_dir=None, q_neu=N
         u = _unflat(_dense_solve(A_factored, b), mesh, source)
         return (u, None) if return_info else u
     shift = 0.0
-    if not bool(np.any(bc == BC_DIRICHLET)):
+    singular = not bool(np.any(bc == BC_DIRICHLET))
+    if iterative.nullspace not in ("shift", "project"):
+        raise ValueError(f"nullspace {iterative.nullspace!r} must be 'shift' or 'project'")
+    if singular:
         torch = _torch()
-        probe = torch.sin(torch.arange(op.n, dtype=torch.float64, device=dev))
-        ones = torch.ones_like(probe)
-        axpby(-dot(probe, ones) / op.n, ones, 1.0, probe)
-        Ap = op.apply(probe)
-        shift = 1.0e-6 * float(np.sqrt(dot(Ap, Ap) / dot(probe, probe)))
+        ones = torch.ones(op.n, dtype=torch.float64, device=dev)
+        if iterative.nullspace == "shift":
+            probe = torch.sin(torch.arange(op.n, dtype=torch.float64, device=dev))
+            axpby(-dot(probe, ones) / op.n, ones, 1.0, probe)
+            Ap = op.apply(probe)
+            shift = 1.0e-6 * float(np.sqrt(dot(Ap, Ap) / dot(probe, probe)))
         axpby(-dot(b, ones) / op.n, ones, 1.0, b)
     x, info = _iterative_solve(mesh, op, b, x0, alpha=0.0, shift=shift, iterative=iterative,
                                preconditioner=preconditioner)
+    if singular and iterative.nullspace == "project":
+        axpby(-dot(x, ones) / op.n, ones, 1.0, x)
     u = _unflat(x, mesh, source)
     return (u, info) if return_info else u
 

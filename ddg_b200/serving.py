@@ -23,6 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
+from .autotune import Tile, TileAutotuner
 from .dg2d.mesh import build_mesh_2d, uniform_rectangle_mesh_2d
 from .dg2d.reference import ref_element
 
@@ -41,6 +42,7 @@ class Request:
     done: float = -1.0
     iterations: int = 0
     status: str = ""
+    precision: str = ""     # "fp32" or "fp64": the pool that served it
     x: np.ndarray | None = field(default=None, repr=False)
 
     @property
@@ -106,25 +108,35 @@ def source_nodal(m, modes):
     return sum(a * np.sin(np.pi * i * m.x) * np.sin(np.pi * j * m.y) for a, i, j in zip(amp, kx, ky))
 
 
-def bytes_per_element(N: int) -> int:
-    """Device bytes a pool element needs (geometry, words, inverses, vectors)."""
+def bytes_per_element(N: int, fp32: bool = False) -> int:
+    """Device bytes a pool element needs (geometry, words, inverses, vectors;
+    a float32 pool adds float32 copies of the geometry and inverses and keeps
+    its iteration vectors in float32)."""
     Np = (N + 1) * (N + 2) // 2
-    return 14 * 8 + 12 + 4 + 8 + Np * (Np + 1) // 2 * 8 + 7 * Np * 8 + 16
+    nS = Np * (Np + 1) // 2
+    base = 14 * 8 + 12 + 4 + 8 + nS * 8 + Np * 8 + 16            # geometry, words, seg, alpha, binv, b
+    if fp32:
+        return base + 14 * 4 + nS * 4 + 6 * Np * 4
+    return base + 6 * Np * 8
 
 
 class SolvePool:
-    """One ``ddg_pool`` (one polynomial degree)."""
+    """One ``ddg_pool`` (one polynomial degree and vector precision)."""
 
-    def __init__(self, N, capacity, max_requests, max_request_K, tau_scale, device=0):
+    def __init__(self, N, capacity, max_requests, max_request_K, tau_scale, device=0, fp32=False):
         self.N = N
+        self.fp32 = fp32
         self.tau_scale = tau_scale
         self.device = device
         self.max_requests = max_requests
         h = C.c_void_p()
-        _lib.check(_lib.lib().ddg_pool_create(N, capacity, max_requests, max_request_K, tau_scale, device,
-                                              C.byref(h)), "ddg_pool_create")
+        _lib.check(_lib.lib().ddg_pool_create_ex(N, capacity, max_requests, max_request_K, tau_scale,
+                                                 _lib.DDG_FP32 if fp32 else _lib.DDG_FP64, device, C.byref(h)),
+                   "ddg_pool_create_ex")
         self._h = h
         self.slot_req = {}
+        self.elements = 0           # elements of the requests admitted and not retired
+        self._tile = None
         self._act = np.zeros(max_requests, dtype=np.int32)
         self._its = np.zeros(max_requests, dtype=np.int32)
 
@@ -148,7 +160,14 @@ class SolvePool:
             return False
         _lib.check(rc, "ddg_pool_admit")
         self.slot_req[slot.value] = (req, mesh)
+        self.elements += mesh.K
+        req.precision = "fp32" if self.fp32 else "fp64"
         return True
+
+    def set_tile(self, tile: Tile):
+        if tile != self._tile:
+            _lib.check(_lib.lib().ddg_pool_set_tile(self._h, tile.threads, tile.persistent), "ddg_pool_set_tile")
+            self._tile = tile
 
     def iterate(self, pairs, stream):
         _lib.check(_lib.lib().ddg_pool_iterate(self._h, pairs, stream), "ddg_pool_iterate")
@@ -160,6 +179,7 @@ class SolvePool:
 
     def retire(self, slot, stream):
         req, mesh = self.slot_req.pop(slot)
+        self.elements -= mesh.K
         x = np.empty((mesh.K, mesh.Np))
         info = _lib.SolveInfo()
         _lib.check(_lib.lib().ddg_pool_retire(self._h, slot, x.ctypes.data, stream, C.byref(info)),
@@ -175,21 +195,43 @@ class SolvePool:
 
 
 class ServingEngine:
-    """Continuous-batching scheduler over one pool per polynomial degree."""
+    """Continuous-batching scheduler over one pool per polynomial degree.
+
+    ``autotune`` (default on): the tile shape of every pool launch (threads
+    per block, persistent grid, iterations per graph) comes from a
+    :class:`~ddg_b200.autotune.TileAutotuner` keyed on (degree, active
+    element count); pass a tuner to share or preload one.  With
+    ``autotune=False`` every launch uses 128 threads, one thread per element
+    and ``pairs``.
+
+    ``fp32_tol`` (default 1e-6): requests whose tolerance is at least this
+    run in a float32 pool of their degree (float32 vectors, geometry and
+    inverses; float64 reductions), the others in the float64 pool; None
+    keeps every request in float64."""
 
     def __init__(self, degrees=(2, 3, 4), hbm_budget_bytes=120e9, tau_scale=0.5, max_requests=4096,
-                 max_request_K=2 * 96 * 96, capacity=None, pairs=4, device=0):
+                 max_request_K=2 * 96 * 96, capacity=None, pairs=4, device=0, autotune=True, fp32_tol=1e-6):
         import torch
         torch.cuda.set_device(device)
         self.device = device
         self.tau_scale = tau_scale
         self.pairs = pairs
+        if autotune is True:
+            self.tuner = TileAutotuner()
+        elif autotune:
+            self.tuner = autotune
+        else:
+            self.tuner = None
         self.meshes = _MeshCache()
+        self.fp32_tol = fp32_tol
         self.pools = {}
-        share = hbm_budget_bytes / len(degrees)
+        kinds = (False, True) if fp32_tol is not None else (False,)
+        share = hbm_budget_bytes / (len(degrees) * len(kinds))
         for N in degrees:
-            cap = int(min(share // bytes_per_element(N), 32_000_000)) if capacity is None else int(capacity)
-            self.pools[N] = SolvePool(N, cap, max_requests, max_request_K, tau_scale, device)
+            for f32 in kinds:
+                cap = (int(min(share // bytes_per_element(N, f32), 32_000_000)) if capacity is None
+                       else int(capacity))
+                self.pools[(N, f32)] = SolvePool(N, cap, max_requests, max_request_K, tau_scale, device, fp32=f32)
         self.stream = torch.cuda.Stream(device=device)
         self._torch = torch
 
@@ -202,29 +244,42 @@ class ServingEngine:
         the finished requests with latency, iterations and solution."""
         s = self.stream.cuda_stream
         pending = deque(sorted(requests, key=lambda r: r.arrival))
-        waiting = {N: deque() for N in self.pools}
+        waiting = {key: deque() for key in self.pools}
         done = []
         t0 = time.perf_counter()
         while len(done) < len(requests):
             now = time.perf_counter() - t0
             while pending and (pending[0].arrival <= now or not realtime):
                 r = pending.popleft()
-                waiting[r.N].append(r)
-            for N, q in waiting.items():              # admit while slots / ranges are free
-                pool = self.pools[N]
+                waiting[(r.N, self.fp32_tol is not None and r.tol >= self.fp32_tol)].append(r)
+            for key, q in waiting.items():            # admit while slots / ranges are free
+                pool = self.pools[key]
                 while q:
-                    m, arrays = self.meshes.get(q[0].n, N)
+                    m, arrays = self.meshes.get(q[0].n, pool.N)
                     if not pool.admit(q[0], m, arrays, s):
                         break
                     q.popleft().admitted = time.perf_counter() - t0
             busy = [p for p in self.pools.values() if p.active]
+            timed = []
             for p in busy:
-                p.iterate(self.pairs, s)
+                tkey = f"N{p.N}-fp32" if p.fp32 else f"N{p.N}"
+                tile = self.tuner.choose(tkey, p.elements) if self.tuner else Tile(128, 0, self.pairs)
+                p.set_tile(tile)
+                if self.tuner:
+                    ev = (self._torch.cuda.Event(enable_timing=True), self._torch.cuda.Event(enable_timing=True))
+                    ev[0].record(self.stream)
+                    p.iterate(tile.pairs, s)
+                    ev[1].record(self.stream)
+                    timed.append((tkey, p.elements, tile, ev))
+                else:
+                    p.iterate(tile.pairs, s)
             for p in busy:
                 for slot in p.finished(s):
                     r = p.retire(slot, s)
                     r.done = time.perf_counter() - t0
                     done.append(r)
+            for tkey, el, tile, ev in timed:   # finished() synchronised the stream
+                self.tuner.record(tkey, el, tile, ev[0].elapsed_time(ev[1]) * 1e-3 / (2 * tile.pairs))
             if not busy and pending and realtime:
                 time.sleep(max(0.0, min(0.002, pending[0].arrival - (time.perf_counter() - t0))))
         self.elapsed = time.perf_counter() - t0
@@ -236,7 +291,8 @@ def summarize(done, elapsed):
     return {"requests": len(done), "elapsed_s": elapsed, "solves_per_s": len(done) / elapsed,
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "mean_iterations": float(np.mean([r.iterations for r in done])),
-            "converged": int(sum(r.status == "converged" for r in done))}
+            "converged": int(sum(r.status == "converged" for r in done)),
+            "fp32_requests": int(sum(r.precision == "fp32" for r in done))}
 
 
 def solve_one_at_a_time(requests, tau_scale=0.5):

@@ -109,11 +109,13 @@ int ddg_sipg_apply(ddg_sipg_op *op, int precision, double alpha,
  * with a per-element diffusivity); DDG_ENGINE_CUDA_CORES: plain FMA on the
  * CUDA cores.  Defaults: every float64 apply (ddg_sipg_apply with DDG_FP64,
  * float64 CG and residuals) and stand-alone float32 applies use the tensor
- * cores; float32 CG iterations (ddg_sipg_cg with DDG_FP32,
- * ddg_sipg_cg_mixed) the CUDA cores, whose restarted mixed-precision
- * iterations converge in fewer steps.  Calling this sets all three where
- * the degree has the engine (DDG_ERR_UNSUPPORTED if it has none); the
- * float32 CG default is not restored by a later call.  The host-buffer
+ * cores, and so do float32 CG iterations (ddg_sipg_cg with DDG_FP32,
+ * ddg_sipg_cg_mixed).  Both float32 engines centre each element's values on
+ * its first nodal value before the derivative products, so their rounding
+ * error on smooth vectors scales with the element's variation (the mixed
+ * solver then needs as many iterations as with float64 arithmetic).
+ * Calling this sets all three where the degree has the engine
+ * (DDG_ERR_UNSUPPORTED if it has none).  The host-buffer
  * apply recaptures its pipeline with the new engine on its next call.  No
  * reference counterpart (the reference's operator is jax.grad of its
  * bilinear form, sipg.py:304-337). */
@@ -269,6 +271,12 @@ typedef struct ddg_pool ddg_pool;
  * max_requests: concurrent requests; max_request_K: largest request. */
 int ddg_pool_create(int N, int capacity, int max_requests, int max_request_K,
                     double tau_scale, int device, ddg_pool **out);
+/* The same with the precision of the iteration vectors: DDG_FP64, or
+ * DDG_FP32 (float32 vectors, geometry and block-Jacobi inverses, float64
+ * reductions and CG scalars; for requests whose tolerance float32
+ * iterations reach, such as 1e-6).  No reference counterpart. */
+int ddg_pool_create_ex(int N, int capacity, int max_requests, int max_request_K,
+                       double tau_scale, int precision, int device, ddg_pool **out);
 int ddg_pool_destroy(ddg_pool *pool);
 /* Admit one (alpha M + A) u = J M f solve on `mesh` (host arrays, its own
  * numbering; bc_types as in ddg_sipg_mesh_desc), source f (K x Np,
@@ -279,6 +287,13 @@ int ddg_pool_admit(ddg_pool *pool, const ddg_sipg_mesh_desc *mesh, double alpha,
                    void *stream, int *slot);
 /* 2*pairs block-Jacobi PCG iterations of every active request (one graph). */
 int ddg_pool_iterate(ddg_pool *pool, int pairs, void *stream);
+/* Tile shape of the pool's element kernels in later ddg_pool_iterate calls:
+ * threads per block (64, 128 or 256), persistent 0 (one thread per element)
+ * or 1 (a grid of at most 2048/threads blocks per SM looping over the
+ * elements).  Results are identical for every shape; the serving
+ * autotuner picks the fastest per (degree, element count).  No reference
+ * counterpart (the reference has no serving layer). */
+int ddg_pool_set_tile(ddg_pool *pool, int threads, int persistent);
 /* Per slot: 1 while iterating, 0 when finished or empty; iteration counts. */
 int ddg_pool_poll(ddg_pool *pool, int32_t *active, int32_t *iterations, void *stream);
 /* Copy a finished request's solution (K x Np, host) and free its slot. */

@@ -30,8 +30,12 @@ here is computed by the reference's code path:
   and CG preconditioned by the p- and hp-multigrid V-cycles, with the
   iteration counts the CG loop took.
 
-Outputs: ``refelem.npz``, ``meshes.npz``, ``applies.npz``, ``solves.npz``
-next to this file.
+* one dual-splitting Navier-Stokes step (``incompressible_ns.ns_step_2d``) on
+  the reference test's channel, by direct LU and by multigrid-preconditioned
+  CG, and a second (BDF2) step.
+
+Outputs: ``refelem.npz``, ``meshes.npz``, ``applies.npz``, ``solves.npz``,
+``ins.npz`` next to this file.
 """
 
 from __future__ import annotations
@@ -258,8 +262,44 @@ def main(src: str) -> None:
     out_sol["hpmg/vcycle_out"] = _a(pc(r))
     print(f"hpmg {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
 
+    # ---- one dual-splitting INS step (incompressible_ns.py:509-666) on the
+    # reference test's channel (walls on three sides, outflow on x = 1; 6x6
+    # quads, N = 3, dt = 0.01, nu = 0.02): direct-LU and matrix-free CG with
+    # the p-multigrid preconditioners, then a BDF2 step from the LU result
+    out_ins = {}
+    rins = imp("ddg.dg2d.incompressible_ns")
+    VX, VY, E = rmesh.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 6, 6)
+    m = rmesh.build_mesh_2d(VX, VY, E, 3)
+    isb = boundary_faces(m)
+    xf = _a(m.x)[_a(m.Fmask)]                       # (Nfp, 3, K) face-node x
+    outflow = np.all(np.abs(xf - 1.0) < 1e-7, axis=0).T
+    ins_bc = np.where(isb, np.where(outflow, rins.BC_INS_OUTFLOW, rins.BC_INS_WALL),
+                      rins.BC_INS_INTERIOR).astype(np.int32)
+    dt, nu = 0.01, 0.02
+    zero = np.zeros((int(m.Np), int(m.K)))
+    ux = 0.2 * np.sin(np.pi * _a(m.x)) * np.cos(np.pi * _a(m.y))
+    uy = -0.2 * np.cos(np.pi * _a(m.x)) * np.sin(np.pi * _a(m.y))
+    nxo, nyo = rins.ns_advection_2d(m, ux, uy, ins_bc_types=ins_bc, bc_ux=zero, bc_uy=zero)
+    dpdn0 = np.zeros((3 * int(m.Nfp), int(m.K)))
+    args = (m, ux, uy, ux, uy, nxo, nyo, dpdn0)
+    kw = dict(dt=dt, nu=nu, bdf=rins.BDF1, ins_bc_types=ins_bc, bc_ux=zero, bc_uy=zero)
+    ops = rins.build_ins_operators(m, dt=dt, nu=nu, g0=1.0, ins_bc_types=ins_bc)
+    res_lu = rins.ns_step_2d(*args, ops=ops, **kw)
+    ops_mf = rins.build_ins_operators(m, dt=dt, nu=nu, g0=1.0, ins_bc_types=ins_bc, skip_factor=True)
+    pp, vp = rins.make_ins_mg_preconditioners(m, dt=dt, nu=nu, g0=1.0, ins_bc_types=ins_bc)
+    res_mg = rins.ns_step_2d(*args, ops=ops_mf, iterative=IC(tol=1e-11, maxiter=3000),
+                             pressure_preconditioner=pp, viscous_preconditioner=vp, **kw)
+    ops2 = rins.build_ins_operators(m, dt=dt, nu=nu, g0=rins.BDF2.g0, ins_bc_types=ins_bc)
+    res2 = rins.ns_step_2d(m, res_lu[0], res_lu[1], ux, uy, res_lu[3], res_lu[4], res_lu[5], dt=dt, nu=nu,
+                           bdf=rins.BDF2, ops=ops2, ins_bc_types=ins_bc, bc_ux=zero, bc_uy=zero)
+    out_ins.update(VX=_a(VX), VY=_a(VY), EToV=_a(E), ins_bc=ins_bc, ux0=ux, uy0=uy, Nux_old=_a(nxo), Nuy_old=_a(nyo))
+    for tag, res in (("lu", res_lu), ("mg", res_mg), ("bdf2", res2)):
+        for name, v in zip(("ux", "uy", "p", "Nux", "Nuy", "dpdn"), res):
+            out_ins[f"{tag}/{name}"] = _a(v)
+    print(f"ins done {time.time() - t0:.1f}s", flush=True)
+
     for fname, d in (("refelem.npz", out_ref), ("meshes.npz", out_mesh), ("applies.npz", out_app),
-                     ("solves.npz", out_sol)):
+                     ("solves.npz", out_sol), ("ins.npz", out_ins)):
         np.savez_compressed(os.path.join(HERE, fname), **{k: np.asarray(v) for k, v in d.items()})
     print(f"wrote fixtures in {time.time() - t0:.1f}s")
 

@@ -199,3 +199,24 @@ def test_multigrid_matches_reference():
                                        return_info=True)
     assert abs(info.iterations - int(s["hpmg/cg_iterations"])) <= 4
     assert _rel(u, s["hpmg/u"]) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed-restart"])
+def test_mixed_precision_solve_matches_reference_fp64_solution(precision):
+    """The mixed-precision block-Jacobi PCG (float32 iterations, float64
+    refinement) reaches relative L2 error <= 1e-8 against the reference's own
+    float64 solution of the same Helmholtz system (16x16 quads, N=4, alpha=5,
+    Dirichlet x / Neumann y, tau_scale=0.5, 8-mode RHS)."""
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    s = _load("solves.npz")
+    VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 16, 16)
+    p = pm.build_mesh_2d(VX, VY, E, 4)
+    bc = s["helmholtz16/bc"]
+    pc = ps.make_helmholtz_block_jacobi_preconditioner(p, alpha=5.0, nu=1.0, bc_types=bc, tau_scale=0.5)
+    u, info = ps.solve_sipg_helmholtz_2d(p, s["helmholtz16/rhs"], alpha=5.0, nu=1.0, bc_types=bc, tau_scale=0.5,
+                                         iterative=ps.IterativeConfig(tol=1e-10, maxiter=20000, precision=precision),
+                                         preconditioner=pc, return_info=True)
+    ref = s["helmholtz16/u"]
+    assert info.status == "converged"
+    assert np.linalg.norm(u - ref) / np.linalg.norm(ref) <= 1e-8

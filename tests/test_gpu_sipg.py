@@ -508,3 +508,44 @@ def test_apply_host_follows_engine_switch():
         assert np.array_equal(got, dev), engine
         assert _rel(got, ref) < APPLY_RTOL64
     op.close()
+
+
+@pytest.mark.parametrize("use_pc", [False, True])
+def test_projected_singular_mode_is_exact_mean_free_solution(use_pc):
+    """Pure-Neumann Poisson: nullspace="project" returns the exact solution of
+    the consistent system A u = P b (P = projection onto 1-perp) with zero mean,
+    checked against the oracle's dense bordered solve; the reference's
+    epsilon-shift solution differs from it by a small, stated gap."""
+    from ddg_b200.dg2d import sipg as ps
+    o, p = _pair(6, 5, 3)
+    bc = osp.boundary_bc(o, osp.BC_NEUMANN)
+    src = np.cos(np.pi * o.x) * np.cos(np.pi * o.y) + 0.2 * o.x
+    A = osp.dense_matrix(o, bc_types=bc, tau_scale=200.0)
+    b = osp._rhs(o, src, bc, None, None, 200.0)
+    n = b.size
+    b = b - b.mean()
+    K = np.zeros((n + 1, n + 1))
+    K[:n, :n] = A
+    K[:n, n] = K[n, :n] = 1.0
+    ue = np.linalg.solve(K, np.concatenate([b, [0.0]]))[:n].reshape(o.K, o.Np).T
+    pc = ps.make_sipg_block_jacobi_preconditioner(p, bc_types=bc) if use_pc else None
+    u, info = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, preconditioner=pc, return_info=True,
+                                       iterative=ps.IterativeConfig(tol=1e-12, maxiter=5000, nullspace="project"))
+    assert info.status == "converged"
+    assert abs(u.mean()) < 1e-12 * np.abs(u).max()
+    assert np.linalg.norm(u - ue) / np.linalg.norm(ue) < 1e-9
+    # the reference's epsilon-shift mode solves (A + eps I) u = P b, eps =
+    # 1e-6 ||A probe|| / ||probe||: it matches the dense shifted solve, and its
+    # distance to the exact mean-free solution is the shift's bias
+    # (eps / lambda_1 relative on the slowest mode; about 9 % here, where
+    # tau_scale = 200 makes ||A|| large against lambda_1)
+    probe = np.sin(np.arange(n, dtype=np.float64))
+    probe -= probe.mean()
+    eps = 1e-6 * np.linalg.norm(A @ probe) / np.linalg.norm(probe)
+    ush = np.linalg.solve(A + eps * np.eye(n), b).reshape(o.K, o.Np).T
+    us = ps.solve_sipg_poisson_2d(p, src, bc_types=bc, preconditioner=pc,
+                                  iterative=ps.IterativeConfig(tol=1e-12, maxiter=5000))
+    assert np.linalg.norm(us - ush) / np.linalg.norm(ush) < 1e-8
+    gap = np.linalg.norm(us - ue) / np.linalg.norm(ue)
+    gap_dense = np.linalg.norm(ush - ue) / np.linalg.norm(ue)
+    assert abs(gap - gap_dense) < 1e-6 and gap > 1e-3
