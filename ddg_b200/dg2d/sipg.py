@@ -437,10 +437,24 @@ def solve_sipg_poisson_2d(mesh: Mesh2D, source, *, bc_types, u_dir=None, q_neu=N
             Ap = op.apply(probe)
             shift = 1.0e-6 * float(np.sqrt(dot(Ap, Ap) / dot(probe, probe)))
         axpby(-dot(b, ones) / op.n, ones, 1.0, b)
-    x, info = _iterative_solve(mesh, op, b, x0, alpha=0.0, shift=shift, iterative=iterative,
-                               preconditioner=preconditioner)
     if singular and iterative.nullspace == "project":
+        # CG on the consistent singular system with every preconditioned
+        # residual projected onto 1-perp, so the search directions never pick
+        # up the constant null vector (pAp stays positive); mean-free result
+        torch = _torch()
+        x = torch.zeros_like(b) if x0 is None else _flat(x0, dev)
+
+        def proj(v):
+            z = (v.clone() if preconditioner is None else
+                 torch.as_tensor(preconditioner(v), dtype=torch.float64, device=dev).contiguous())
+            axpby(-dot(z, ones) / op.n, ones, 1.0, z)
+            return z
+        info = _generic_pcg(op, b, x, alpha=0.0, shift=0.0, tol=iterative.tol, atol=iterative.atol,
+                            maxiter=iterative.maxiter, M=proj)
         axpby(-dot(x, ones) / op.n, ones, 1.0, x)
+    else:
+        x, info = _iterative_solve(mesh, op, b, x0, alpha=0.0, shift=shift, iterative=iterative,
+                                   preconditioner=preconditioner)
     u = _unflat(x, mesh, source)
     return (u, info) if return_info else u
 
