@@ -6,6 +6,7 @@
 
 #include <cmath>
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <cstddef>
 #include <map>
@@ -76,8 +77,8 @@ struct CgGraph {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-#ifndef DDG_HOST_CHUNKS
-#define DDG_HOST_CHUNKS 8   // element chunks of the host-buffer apply pipeline
+#ifndef DDG_HOST_PLAN
+#define DDG_HOST_PLAN 1, 1, 1, 1, 1, 1, 1, 1   // relative chunk sizes of the host-buffer apply pipeline
 #endif
 
 // State of the host-buffer apply (ddg_sipg_apply_host), created on first use:
@@ -101,7 +102,9 @@ struct HostIO {
   std::vector<cudaEvent_t> e_in, e_cmp, e_out;
   std::vector<int> need;                 // per piece (2 per chunk), running maximum
   std::vector<int> p_lo, p_hi;           // piece element ranges
-  int nch = 0, chunk = 0;
+  int nch = 0;
+  std::vector<int> bounds;               // chunk c covers elements [bounds[c], bounds[c + 1])
+  int chunk_of(int k) const { return (int)(std::upper_bound(bounds.begin(), bounds.end(), k) - bounds.begin()) - 1; }
   cudaStream_t s_org = nullptr;       // capture origin of the pipeline graph
   cudaGraphExec_t gexec = nullptr;    // the captured pipeline for (g_u, g_y, g_alpha)
   const double* g_u = nullptr;
@@ -259,11 +262,12 @@ int check_status(ddg_sipg_op* op) {
   return DDG_OK;
 }
 
+// Two CG iterations (the p ping-pong) of the loop body on stream st: with
+// has_cond the step kernel also sets the graph's loop condition.
 template <typename T>
-int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGraphConditionalHandle h) {
+cudaError_t issue_body(ddg_sipg_op* op, const GraphKey& key, cudaStream_t st, int has_cond,
+                       cudaGraphConditionalHandle h) {
   Work& w = op->w[key.prec];
-
-  CK(cudaStreamBeginCaptureToGraph(op->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   ApplyArgs<T> a = apply_args<T>(op);
   a.alpha = key.alpha;
   a.shift = key.shift;
@@ -281,7 +285,7 @@ int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGra
   c.partC = op->partC;
   c.K = op->K;
   c.dev_status = op->status;
-  c.has_cond = 1;
+  c.has_cond = has_cond;
   c.bulk = 1;  // workspace vectors come from cudaMalloc (256-byte aligned)
   c.cond = h;
   cudaError_t e = cudaSuccess;
@@ -298,23 +302,30 @@ int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGra
         // apply of the formed direction with the p.Ap reduction: its
         // neighbour gathers read one vector instead of two
         e = launch_pupd((int64_t)op->K * op->Np, (const float*)c.z, (const float*)pin, (float*)pout, op->ctl,
-                        op->cap);
+                        st);
         if (e == cudaSuccess) {
           a.in0 = (const T*)pout;
           a.in1 = nullptr;
           a.out1 = nullptr;
-          e = launch_apply_tc(op->N, AM_PDOT, a, op->tc_img, op->cap);
+          e = launch_apply_tc(op->N, AM_PDOT, a, op->tc_img, st);
         }
       } else {
-        e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+        e = launch_apply<T>(op->N, AM_PFUSE, a, st);
       }
     } else {
-      e = launch_apply<T>(op->N, AM_PFUSE, a, op->cap);
+      e = launch_apply<T>(op->N, AM_PFUSE, a, st);
     }
     if (e != cudaSuccess) break;
     c.p = (const T*)pout;
-    e = launch_cg_step<T>(op->N, key.pc != 0, false, c, op->cap);
+    e = launch_cg_step<T>(op->N, key.pc != 0, false, c, st);
   }
+  return e;
+}
+
+template <typename T>
+int capture_body(ddg_sipg_op* op, const GraphKey& key, cudaGraph_t body, cudaGraphConditionalHandle h) {
+  CK(cudaStreamBeginCaptureToGraph(op->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t e = issue_body<T>(op, key, op->cap, 1, h);
   cudaGraph_t out = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(op->cap, &out);
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("CG body capture: ") + cudaGetErrorString(e));
@@ -623,12 +634,23 @@ int hio_prepare(ddg_sipg_op* op) {
   if (!op->hio) {
     HostIO* h = new HostIO();
     op->hio = h;  // released by free_op even when set-up stops halfway
-    // pitched copies of 15 rows lose bandwidth as chunks shrink, and copies in
-    // both directions overlap best with few large chunks (measured on B200:
-    // 4-8 chunks of 1.9-3.9 MB); the chunk pipeline needs at least a few
-    h->nch = std::max(1, std::min(DDG_HOST_CHUNKS, K / 4096));
-    h->chunk = ((K + h->nch - 1) / h->nch + 63) / 64 * 64;  // element ranges start on 64-element tiles
-    h->nch = (K + h->chunk - 1) / h->chunk;
+    // chunk plan (relative sizes of consecutive element chunks), measured on
+    // B200 for the 16 MB-per-direction workload: 8 equal chunks 0.52 ms per
+    // call; 4 equal 0.56; small first and last chunks (1,3,4,4,3,1 /
+    // 1,2,2,2,2,2,2,1 / 1,3,3,1) 0.53-0.55; 16 equal 0.62
+    std::vector<int> wts = {DDG_HOST_PLAN};
+    int tot = 0;
+    for (int x : wts) tot += x;
+    if (K < 4096 * (int)wts.size()) wts.assign(1, 1), tot = 1;
+    h->bounds.assign(1, 0);
+    int acc = 0;
+    for (size_t c = 0; c < wts.size(); ++c) {
+      acc += wts[c];
+      int b = c + 1 == wts.size() ? K : (int)((int64_t)K * acc / tot) / 64 * 64;  // 64-element tiles
+      if (b > h->bounds.back()) h->bounds.push_back(b);
+    }
+    if (h->bounds.back() != K) h->bounds.back() = K;
+    h->nch = (int)h->bounds.size() - 1;
     const size_t bytes = (size_t)K * op->Np * sizeof(double);
     CK(cudaMalloc((void**)&h->d_u, bytes));
     CK(cudaMalloc((void**)&h->d_y, bytes));
@@ -650,15 +672,15 @@ int hio_prepare(ddg_sipg_op* op) {
     // mx[k]: the last chunk element k reads (its own, or a neighbour's through
     // a face whose own-interior or neighbour-side bit is set)
     std::vector<int> mx(K);
-    for (int k = 0; k < K; ++k) mx[k] = k / h->chunk;
+    for (int k = 0; k < K; ++k) mx[k] = h->chunk_of(k);
     for (int f = 0; f < 3; ++f)
       for (int k = 0; k < K; ++k) {
         const uint32_t w = op->nbr_host[(size_t)f * K + k];
-        if (w & (32u | 64u)) mx[k] = std::max(mx[k], (int)(w >> 7) / h->chunk);
+        if (w & (32u | 64u)) mx[k] = std::max(mx[k], h->chunk_of((int)(w >> 7)));
       }
     std::vector<int> need(2 * h->nch), lo(2 * h->nch), hi(2 * h->nch);
     for (int c = 0; c < h->nch; ++c) {
-      const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
+      const int c0 = h->bounds[c], c1 = h->bounds[c + 1];
       int p = c0;
       while (p < c1 && mx[p] <= c) ++p;
       if (p < c1) p = c0 + (p - c0) / 16 * 16;  // ranges of the tensor-core kernel start on 16-element blocks
@@ -727,7 +749,7 @@ int hio_issue(ddg_sipg_op* op, double alpha, const double* src, double* dst, cud
   a.use_tma = aligned16(h->e_u) && aligned16(h->e_y);
   int next = 0;
   for (int c = 0; c < h->nch; ++c) {
-    const int c0 = c * h->chunk, c1 = std::min(K, c0 + h->chunk);
+    const int c0 = h->bounds[c], c1 = h->bounds[c + 1];
     const size_t w = (size_t)(c1 - c0) * sizeof(double);
     CK(cudaMemcpy2DAsync(h->d_u + c0, pitch, src + c0, pitch, w, Np, cudaMemcpyHostToDevice, h->s_in));
     CK(cudaEventRecord(h->e_in[c], h->s_in));
@@ -930,9 +952,18 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
   cudaStream_t s = (cudaStream_t)stream;
   GraphKey key{prec, cfg->pc, cfg->alpha, cfg->shift};
   key.engine = prec == DDG_FP32 ? (op->tc_img ? op->cg32_engine : DDG_ENGINE_CUDA_CORES) : op->fp64_engine;
+  // DDG_CG_EAGER=1: launch the iteration kernels directly, checking the loop
+  // flag from the host every 16 iterations, instead of the conditional graph
+  // (same kernels and results; profilers cannot see into conditional graphs)
+  static const bool eager = [] {
+    const char* v = std::getenv("DDG_CG_EAGER");
+    return v && v[0] == '1';
+  }();
   CgGraph* gr = nullptr;
-  rc = get_graph(op, key, &gr);
-  if (rc != DDG_OK) return rc;
+  if (!eager) {
+    rc = get_graph(op, key, &gr);
+    if (rc != DDG_OK) return rc;
+  }
 
   CgCtl h{};
   h.tol2 = cfg->tol * cfg->tol;
@@ -991,7 +1022,23 @@ extern "C" int ddg_sipg_cg(ddg_sipg_op* op, const ddg_cg_config* cfg, const void
     if (e == cudaSuccess) e = launch_cg_step<float>(op->N, cfg->pc != 0, true, c, s);
   }
   if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("CG init launch: ") + cudaGetErrorString(e));
-  CK(cudaGraphLaunch(gr->exec, s));
+  if (eager) {
+    // every kernel returns at once when the loop flag is down, and the step
+    // lowers it at maxiter, so the loop ends within 16 iterations of that
+    for (int it = 0; it < cfg->maxiter + 16; it += 2) {
+      e = prec == DDG_FP64 ? issue_body<double>(op, key, s, 0, cudaGraphConditionalHandle{})
+                           : issue_body<float>(op, key, s, 0, cudaGraphConditionalHandle{});
+      if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("CG iteration launch: ") + cudaGetErrorString(e));
+      if (it % 16 == 14) {
+        int cont = 0;
+        CK(cudaMemcpyAsync(&cont, &op->ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (!cont) break;
+      }
+    }
+  } else {
+    CK(cudaGraphLaunch(gr->exec, s));
+  }
   CK(cudaMemcpyAsync(x, w.x, w.bytes, cudaMemcpyDeviceToDevice, s));
   CgCtl res{};
   CK(cudaMemcpyAsync(&res, op->ctl, sizeof(res), cudaMemcpyDeviceToHost, s));

@@ -187,7 +187,10 @@ typedef struct {
  * maxiter iterations.  b, x: device vectors of the config's precision;
  * x holds x0 on entry and the solution on exit.  The whole loop runs on the
  * device as a CUDA graph with a conditional while node; the call returns
- * after the stream has been synchronised and `info` filled. */
+ * after the stream has been synchronised and `info` filled.  With the
+ * environment variable DDG_CG_EAGER=1 the same iteration kernels are
+ * launched directly and the loop flag is read every 16 iterations (for
+ * profilers, which cannot see kernels inside conditional graphs). */
 int ddg_sipg_cg(ddg_sipg_op *op, const ddg_cg_config *cfg, const void *b,
                 void *x, void *stream, ddg_solve_info *info);
 
