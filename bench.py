@@ -480,6 +480,63 @@ def profile_apply(args):
     print(f"{args.profile_reps} {args.profile_apply} applies done", flush=True)
 
 
+def profile_kernels(args):
+    """Short runs of the other kernels for a profiler's per-kernel captures:
+    `cg-fp64` / `cg-fp32`: block-Jacobi PCG on the workload with the
+    iteration kernels launched eagerly (DDG_CG_EAGER=1, which the caller
+    sets; conditional graphs hide their kernels from profilers), including
+    the block-Jacobi set-up; `mg`: V-cycle applies of the pressure-Poisson
+    workload's hp-multigrid; `serving`: a 64-request stream through the
+    pools; `adjoint`: one gradient of the differentiation workload."""
+    import torch
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    what = args.profile_kernels
+    if what.startswith("cg-"):
+        m, bc, f = workload_arrays(pm.build_mesh_2d, pm.uniform_rectangle_mesh_2d)
+        op = m.device_operator(bc, TAU_SCALE)
+        op.pc_build(ALPHA)
+        dt = torch.float64 if what == "cg-fp64" else torch.float32
+        b = torch.as_tensor(f.T.reshape(-1).copy(), device="cuda").to(dt)
+        x = torch.zeros_like(b)
+        st = op.cg(b, x, tol=1e-12, maxiter=args.profile_maxiter, pc=True, alpha=ALPHA,
+                   precision="fp64" if what == "cg-fp64" else "fp32")
+        print(what, st, flush=True)
+    elif what == "mg":
+        from ddg_b200.dg2d import multigrid as pmg
+        VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 2.0, 16, 32)
+        base = pm.build_mesh_2d(VX, VY, E, 3)
+
+        def nbc(mm):
+            return np.where(mm.EToE == np.arange(mm.K)[:, None], ps.BC_NEUMANN, 0).astype(np.int32)
+        mg, fin = pmg.make_sipg_hpmg_preconditioner(base, 3, bc_fn=nbc, regularize=True, tau_scale=TAU_SCALE)
+        v = torch.randn(fin.K * fin.Np, dtype=torch.float64, device="cuda")
+        mg.apply_device(v)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()    # the V-cycles only (not the set-up's probing)
+        for _ in range(args.profile_reps):
+            mg.apply_device(v)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        print("mg done", flush=True)
+    elif what == "serving":
+        from ddg_b200 import serving
+        eng = serving.ServingEngine(degrees=(2, 3, 4), capacity=1_000_000, max_requests=128, pairs=4)
+        done = eng.run(serving.make_requests(count=64, seed=0), realtime=False)
+        eng.close()
+        print("serving", len(done), flush=True)
+    elif what == "adjoint":
+        from ddg_b200 import adjoint
+        VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 64, 64)
+        m = pm.build_mesh_2d(VX, VY, E, 4)
+        bc = np.where(m.EToE == np.arange(m.K)[:, None], 1, 0).astype(np.int32)
+        op = m.device_operator(bc, TAU_SCALE)
+        f = torch.as_tensor((np.sin(np.pi * m.x) * np.sin(np.pi * m.y)).T.reshape(-1).copy(), device="cuda")
+        G = torch.as_tensor(0.5 * np.random.default_rng(2).standard_normal((1, m.K)), device="cuda")
+        L, grads, its = adjoint.loss_and_grad(op, G, f, torch.zeros_like(f), tol=1e-8, maxiter=4000)
+        print("adjoint", its, flush=True)
+
+
 def profile_solves(args):
     """One float64 and one mixed block-Jacobi PCG solve of the workload."""
     import torch
@@ -575,6 +632,8 @@ def main():
     ap.add_argument("--profile-apply", choices=["fp64", "fp32"], default=None,
                     help="only stand-alone applies of one precision (for a profiler's capture of that kernel)")
     ap.add_argument("--profile-reps", type=int, default=5)
+    ap.add_argument("--profile-kernels", choices=["cg-fp64", "cg-fp32", "mg", "serving", "adjoint"], default=None,
+                    help="only a short run of those kernels (for a profiler's per-kernel capture)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -584,6 +643,9 @@ def main():
         return
     if args.profile_apply:
         profile_apply(args)
+        return
+    if args.profile_kernels:
+        profile_kernels(args)
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)

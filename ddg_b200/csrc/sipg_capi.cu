@@ -301,23 +301,35 @@ cudaError_t issue_body(ddg_sipg_op* op, const GraphKey& key, cudaStream_t st, in
         // the direction first (one streaming pass), then the tensor-core
         // apply of the formed direction with the p.Ap reduction: its
         // neighbour gathers read one vector instead of two
+        // (programmatic dependent launches: each kernel waits for its
+        // predecessor on the device, so launches overlap the previous tail)
         e = launch_pupd((int64_t)op->K * op->Np, (const float*)c.z, (const float*)pin, (float*)pout, op->ctl,
-                        st);
+                        st, has_cond);
         if (e == cudaSuccess) {
           a.in0 = (const T*)pout;
           a.in1 = nullptr;
           a.out1 = nullptr;
+          a.pdl = has_cond;
           e = launch_apply_tc(op->N, AM_PDOT, a, op->tc_img, st);
+          a.pdl = 0;
+          c.pdl = has_cond;
         }
       } else {
         e = launch_apply<T>(op->N, AM_PFUSE, a, st);
       }
     } else {
+      // float64 on the FP64 tensor cores: programmatic dependent launches
+      // as in the float32 body (the CUDA-core kernel keeps plain launches)
+      const bool dm = key.engine == DDG_ENGINE_TENSOR_CORES && op->dm_img;
+      a.pdl = dm ? has_cond : 0;
       e = launch_apply<T>(op->N, AM_PFUSE, a, st);
+      a.pdl = 0;
+      c.pdl = dm ? has_cond : 0;
     }
     if (e != cudaSuccess) break;
     c.p = (const T*)pout;
     e = launch_cg_step<T>(op->N, key.pc != 0, false, c, st);
+    c.pdl = 0;
   }
   return e;
 }

@@ -113,6 +113,12 @@ constexpr uint32_t NBR_MAX_K = (1u << 25) - 1u;
 enum DevStatus : unsigned int { ST_TMA_TIMEOUT = 1u, ST_BAD_INDEX = 2u };
 
 // ------------------------------------------------------- PTX helpers (TMA)
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the previous kernel's last CTAs drain; it
+// waits here, before touching anything that kernel wrote (returns at once
+// for an ordinary launch).
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(BLOCK, (N <= 4 ? 2 : 1)) k_apply_dm(ApplyArgs<
   __shared__ double s_red[64];
   __shared__ int s_ok;
 
+  grid_dep_wait();
   if (MODE == AM_PFUSE && a.ctl->cont == 0) return;  // uniform across the grid
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -575,8 +576,8 @@ cudaError_t launch_one(const ApplyArgs<double>& a, cudaStream_t s) {
   const int nrb = ranged ? (a.k_hi + RB - 1) / RB - a.k_lo / RB : (a.K + RB - 1) / RB;
   if (nrb <= 0) return cudaSuccess;
   const int grid = std::max(1, std::min((nrb + WARPS - 1) / WARPS, nb * sm_count()));
-  k_apply_dm<N, MODE><<<grid, BLOCK, shape_of(N).smem, s>>>(a);
-  return cudaGetLastError();
+  PdlLaunch l(dim3(grid), dim3(BLOCK), shape_of(N).smem, s, a.pdl);
+  return cudaLaunchKernelEx(&l.cfg, k_apply_dm<N, MODE>, a);
 }
 template <int N>
 cudaError_t launch_n(int mode, const ApplyArgs<double>& a, cudaStream_t s) {

@@ -437,6 +437,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step_bulk(CgArgs<T> a) {
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ double s_red[64];
   __shared__ int s_ok;
+  grid_dep_wait();
   if (a.ctl->cont == 0) {
     if (a.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
     return;
@@ -1135,7 +1136,8 @@ static void launch_cg_one(const CgArgs<T>& a, cudaStream_t s) {
   if (!INIT && a.bulk) {
     // regular iteration with aligned vectors: tiles staged by bulk copies
     constexpr int BB = sizeof(T) == 8 ? 64 : 128;  // four tiles within the 48 KB of static shared memory
-    k_cg_step_bulk<N, T, PC, BB><<<(a.K + BB - 1) / BB, BB, 0, s>>>(a);
+    PdlLaunch l(dim3((a.K + BB - 1) / BB), dim3(BB), 0, s, a.pdl);
+    cudaLaunchKernelEx(&l.cfg, k_cg_step_bulk<N, T, PC, BB>, a);
     return;
   }
   constexpr int B = 128;
@@ -1243,6 +1245,7 @@ cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, doubl
 // step; the same rounding as the fused direction update of the applies
 __global__ void k_pupd(int64_t n, const float* __restrict__ z, const float* __restrict__ p_old,
                        float* __restrict__ p, const CgCtl* ctl) {
+  grid_dep_wait();
   if (ctl->cont == 0) return;
   const float zc = (float)ctl->zcoef, be = (float)ctl->beta;
   const int64_t n4 = n / 4;
@@ -1260,9 +1263,10 @@ __global__ void k_pupd(int64_t n, const float* __restrict__ z, const float* __re
   for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     p[i] = fmaf(zc, z[i], be * p_old[i]);
 }
-cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s) {
-  k_pupd<<<vec_grid((n + 3) / 4), 256, 0, s>>>(n, z, p_old, p, ctl);
-  return cudaGetLastError();
+cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s,
+                        int pdl) {
+  PdlLaunch l(dim3(vec_grid((n + 3) / 4)), dim3(256), 0, s, pdl);
+  return cudaLaunchKernelEx(&l.cfg, k_pupd, n, z, p_old, p, ctl);
 }
 
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s) {

@@ -37,6 +37,7 @@ struct ApplyArgs {
   const double* dm_img;     // float64: FP64 tensor-core operand image (null: CUDA cores)
   const double* dm_geo;     // float64: that kernel's element and face coefficients ([D_COUNT][ldg])
   int k_lo, k_hi;           // AM_APPLY: elements [k_lo, k_hi) only (k_hi = 0: all; k_lo a multiple of 16)
+  int pdl;                  // launch with programmatic stream serialization (CG graph bodies)
 };
 
 template <typename T>
@@ -59,6 +60,7 @@ struct CgArgs {
   int has_cond;
   cudaGraphConditionalHandle cond;
   int bulk;        // x, p, r, Ap, z 16-byte aligned: stage tiles by bulk copies
+  int pdl;         // launch with programmatic stream serialization (CG graph bodies)
 };
 
 struct BlockArgs {
@@ -169,7 +171,23 @@ cudaError_t launch_grad_kappa(int N, const GradArgs& a, cudaStream_t s);
 cudaError_t launch_axpby(int64_t n, double al, const double* x, double be, double* y, cudaStream_t s);
 cudaError_t launch_cast(int64_t n, int to_prec, const void* src, void* dst, cudaStream_t s);
 // float32 CG direction p = zc z + beta p_old (16-byte aligned vectors)
-cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s);
+cudaError_t launch_pupd(int64_t n, const float* z, const float* p_old, float* p, const CgCtl* ctl, cudaStream_t s,
+                        int pdl = 0);
+// launch configuration with programmatic stream serialization when pdl != 0
+struct PdlLaunch {
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  PdlLaunch(dim3 grid, dim3 block, size_t smem, cudaStream_t s, int pdl) {
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+  }
+};
 // r32 = float(r64), x32 = 0, ctl->bb = r32.r32 (reliable-update restart)
 cudaError_t launch_cast_norm(int64_t n, const double* r64, float* r32, float* x32, double* part, CgCtl* ctl,
                              cudaStream_t s);

@@ -240,6 +240,7 @@ __global__ void __launch_bounds__(128, TcDim<N>::CTAS_PER_SM) k_apply_tc(TcArgs 
   __shared__ uint32_t s_taddr;
   __shared__ double s_red[64];
 
+  grid_dep_wait();
   if (DOT && a.ctl->cont == 0) return;  // the loop has stopped (uniform)
   const RefMats<N, float>& R = CRef<N, float>::get();
   const RefPairs<N>& P = CPairs<N>::get();
@@ -749,8 +750,8 @@ static cudaError_t launch_tc_n(const ApplyArgs<float>& a, const uint8_t* img, cu
   t.tau = (float)a.tau;
   t.alpha = (float)a.alpha;
   t.shift = (float)a.shift;
-  tc::k_apply_tc<N, MODE><<<grid, 128, tc_smem_request<N, MODE>(), s>>>(t);
-  return cudaGetLastError();
+  PdlLaunch l(dim3(grid), dim3(128), tc_smem_request<N, MODE>(), s, a.pdl);
+  return cudaLaunchKernelEx(&l.cfg, tc::k_apply_tc<N, MODE>, t);
 }
 
 template <int MODE>
