@@ -21,4 +21,4 @@ literal bilinear form differentiated by torch autograd (the stand-in for
 gather/scatter restatement must agree to 1e-13.
 """
 
-from . import refelem, mesh, sipg, multigrid, refinement  # noqa: F401
+from . import refelem, mesh, sipg, multigrid, refinement, cubature, curved  # noqa: F401

@@ -75,11 +75,17 @@ def _unface(mesh, a):
 
 # ----------------------------------------------------- the operator -------
 
-def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
+def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None, cub=None):
     """Explicit ``sipg_apply_2d`` (``sipg.py:304-337``): d a(u, v) / d v at
     v = 0, including the affine Dirichlet offset when ``u_dir`` is given.
 
     ``u`` is (Np, K) or (Np, K, B); the result has the same shape.
+
+    ``cub`` (an ``oracle.cubature.MeshCubature``) selects the curved-element
+    branch (``sipg.py:190-201`` volume, ``sipg.py:281-299`` faces): the
+    volume integral at the cubature points with their geometric factors, the
+    face integrals at the 1D face points with the surface Jacobian there
+    (normals, tau and the traces stay nodal).
 
     ``kappa`` (K,) is the per-element diffusivity extension (no reference
     counterpart): volume kappa_k grad u . grad v, face averages
@@ -103,11 +109,27 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
     ux = rx * ur + sx * us
     uy = ry * ur + sy * us
 
-    # volume term sum J*(ux*(M vx) + uy*(M vy))  (sipg.py:189)
-    cx = np.einsum("ji,jkb->ikb", M, kvol * J * ux)     # M^T (kappa J ux)
-    cy = np.einsum("ji,jkb->ikb", M, kvol * J * uy)
-    gx = cx.copy()                                       # dL/dvx (per node)
-    gy = cy.copy()
+    if cub is None:
+        # volume term sum J*(ux*(M vx) + uy*(M vy))  (sipg.py:189)
+        cx = np.einsum("ji,jkb->ikb", M, kvol * J * ux)     # M^T (kappa J ux)
+        cy = np.einsum("ji,jkb->ikb", M, kvol * J * uy)
+        gx = cx.copy()                                       # dL/dvx (per node)
+        gy = cy.copy()
+        yvol = 0.0
+    else:
+        if kappa is not None:
+            raise ValueError("kappa is not defined for the cubature branch")
+        # sum_q w J (ux_q vx_q + uy_q vy_q)  (sipg.py:191-201)
+        urq = np.einsum("qi,ikb->qkb", cub.Drq, U)
+        usq = np.einsum("qi,ikb->qkb", cub.Dsq, U)
+        crx, csx, cry, csy = (a[:, :, None] for a in (cub.rx, cub.sx, cub.ry, cub.sy))
+        wJ = (cub.w[:, None] * cub.J)[:, :, None]
+        uxq = crx * urq + csx * usq
+        uyq = cry * urq + csy * usq
+        yvol = (np.einsum("qi,qkb->ikb", cub.Drq, wJ * (crx * uxq + cry * uyq))
+                + np.einsum("qi,qkb->ikb", cub.Dsq, wJ * (csx * uxq + csy * uyq)))
+        gx = np.zeros_like(U)
+        gy = np.zeros_like(U)
 
     # traces (sipg.py:204-249)
     uf, uxf, uyf = _flat(U), _flat(ux), _flat(uy)
@@ -136,13 +158,25 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
     Fs1 = _face(mesh, mesh.Fscale.reshape(-1, order="F"))[0]
     tau = tau_scale * (mesh.N + 1) * (mesh.N + 1) * Fs1
     avgF, jmpF = _face(mesh, avg), _face(mesh, jmp)                   # (Nfp,3,K,B)
-    wsJ = (w * sJ1)[None, :, :, None]
-    wtsJ = (w * tau * sJ1)[None, :, :, None] * kF[0][None, :, :, None]
-    # d/d(jmp_v): -w sJ m1d^T avg + w tau kappa_F sJ m1d^T jmp   (sipg.py:270-279)
-    dj = (-wsJ * np.einsum("fpq,pfkb->qfkb", m1d, avgF)
-          + wtsJ * np.einsum("fpq,pfkb->qfkb", m1d, jmpF))
-    # d/d(avg_v): -w sJ m1d^T jmp_u
-    da = -wsJ * np.einsum("fpq,pfkb->qfkb", m1d, jmpF)
+    if cub is None:
+        wsJ = (w * sJ1)[None, :, :, None]
+        wtsJ = (w * tau * sJ1)[None, :, :, None] * kF[0][None, :, :, None]
+        # d/d(jmp_v): -w sJ m1d^T avg + w tau kappa_F sJ m1d^T jmp   (sipg.py:270-279)
+        dj = (-wsJ * np.einsum("fpq,pfkb->qfkb", m1d, avgF)
+              + wtsJ * np.einsum("fpq,pfkb->qfkb", m1d, jmpF))
+        # d/d(avg_v): -w sJ m1d^T jmp_u
+        da = -wsJ * np.einsum("fpq,pfkb->qfkb", m1d, jmpF)
+    else:
+        # face cubature (sipg.py:284-299): traces interpolated by face_L1d,
+        # weights face_w * face_sJ * w at the face points
+        L1 = cub.face_L1d                                              # (3, Nq, Nfp)
+        Wq = (cub.face_w[:, None, None] * np.transpose(cub.face_sJ, (1, 0, 2))
+              * w[None, :, :])[:, :, :, None]                          # (Nq, 3, K, 1)
+        avq = np.einsum("fqp,pfkb->qfkb", L1, avgF)
+        jmq = np.einsum("fqp,pfkb->qfkb", L1, jmpF)
+        tq = tau[None, :, :, None]
+        dj = np.einsum("fqp,qfkb->pfkb", L1, Wq * (-avq + tq * jmq))
+        da = -np.einsum("fqp,qfkb->pfkb", L1, Wq * jmq)
     dj, da = _unface(mesh, dj), _unface(mesh, da)
 
     yf = np.zeros((K * Np, B))
@@ -161,17 +195,18 @@ def apply(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
 
     gx = gx + _unflat(gxf, Np, K)
     gy = gy + _unflat(gyf, Np, K)
-    y = _unflat(yf, Np, K)
+    y = _unflat(yf, Np, K) + yvol
     y = y + np.einsum("ji,jkb->ikb", Dr, rx * gx + ry * gy) \
           + np.einsum("ji,jkb->ikb", Ds, sx * gx + sy * gy)
     return y[:, :, 0] if squeeze else y
 
 
-def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
+def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None, cub=None):
     """Literal restatement of ``sipg_bilinear_form`` (``sipg.py:142-301``,
-    affine ``cub=None`` branch) on torch float64 tensors; ``kappa`` (a (K,)
-    tensor, may require grad) adds the diffusivity extension described in
-    :func:`apply` (kappa = 1 is the reference form)."""
+    both the nodal ``cub=None`` branch and the cubature branch) on torch
+    float64 tensors; ``kappa`` (a (K,) tensor, may require grad) adds the
+    diffusivity extension described in :func:`apply` (kappa = 1 is the
+    reference form; nodal branch only)."""
     import torch
     ref = mesh.ref
     T = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float64)  # noqa: E731
@@ -183,7 +218,16 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, ka
     vx = rx * (Dr @ v) + sx * (Ds @ v)
     vy = ry * (Dr @ v) + sy * (Ds @ v)
     kap = torch.ones(K, dtype=torch.float64) if kappa is None else kappa
-    vol = torch.sum(kap[None, :] * J * (ux * (M @ vx) + uy * (M @ vy)))
+    if cub is None:
+        vol = torch.sum(kap[None, :] * J * (ux * (M @ vx) + uy * (M @ vy)))
+    else:
+        Drq, Dsq = T(cub.Drq), T(cub.Dsq)
+        crx, csx, cry, csy = T(cub.rx), T(cub.sx), T(cub.ry), T(cub.sy)
+        uxq = crx * (Drq @ u) + csx * (Dsq @ u)
+        uyq = cry * (Drq @ u) + csy * (Dsq @ u)
+        vxq = crx * (Drq @ v) + csx * (Dsq @ v)
+        vyq = cry * (Drq @ v) + csy * (Dsq @ v)
+        vol = torch.sum(T(cub.w)[:, None] * T(cub.J) * (uxq * vxq + uyq * vyq))
     fl = lambda a: a.T.reshape(-1)  # noqa: E731
     vM, vP = torch.as_tensor(mesh.vmapM), torch.as_tensor(mesh.vmapP)
     nx = T(mesh.nx.reshape(-1, order="F"))
@@ -213,6 +257,14 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, ka
     Fs1 = T(mesh.Fscale.reshape((Nfp, 3, K), order="F")[0])
     tau = tau_scale * (mesh.N + 1) * (mesh.N + 1) * Fs1
     wt = T(w)
+    if cub is not None:
+        L1 = T(cub.face_L1d)
+        q = lambda a: torch.einsum("fqp,pfk->qfk", L1, tf(a))  # noqa: E731
+        W = T(cub.face_w)[:, None, None] * T(np.transpose(cub.face_sJ, (1, 0, 2))) * wt[None]
+        cons = -torch.sum(W * q(aDu) * q(jv))
+        adj = -torch.sum(W * q(ju) * q(aDv))
+        pen = torch.sum(W * tau[None] * q(ju) * q(jv))
+        return vol + cons + adj + pen
     wsJ = wt * sJ1
     cons = -torch.einsum("fk,pfk,fpq,qfk->", wsJ, tf(aDu), m1d, tf(jv))
     adj = -torch.einsum("fk,pfk,fpq,qfk->", wsJ, tf(ju), m1d, tf(aDv))
@@ -220,14 +272,15 @@ def bilinear_form_torch(mesh, u, v, *, bc_types, u_dir=None, tau_scale=200.0, ka
     return vol + cons + adj + pen
 
 
-def apply_autograd(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None):
+def apply_autograd(mesh, u, *, bc_types, u_dir=None, tau_scale=200.0, kappa=None, cub=None):
     """``sipg_apply_2d`` exactly as the reference computes it: the gradient
     of the scalar form w.r.t. v at v = 0 (``sipg.py:329-337``)."""
     import torch
     ut = torch.as_tensor(np.asarray(u), dtype=torch.float64)
     v = torch.zeros_like(ut, requires_grad=True)
     kt = None if kappa is None else torch.as_tensor(np.asarray(kappa), dtype=torch.float64)
-    a = bilinear_form_torch(mesh, ut, v, bc_types=bc_types, u_dir=u_dir, tau_scale=tau_scale, kappa=kt)
+    a = bilinear_form_torch(mesh, ut, v, bc_types=bc_types, u_dir=u_dir, tau_scale=tau_scale, kappa=kt,
+                            cub=cub)
     (g,) = torch.autograd.grad(a, v)
     return g.numpy()
 
@@ -248,14 +301,18 @@ def grad_kappa(mesh, u, lam, *, bc_types, tau_scale=200.0, kappa=None):
     return g.numpy()
 
 
-def mass_apply(mesh, u):
-    """J * (M_ref u), ``sipg.py:565,597,853``."""
+def mass_apply(mesh, u, cub=None):
+    """J * (M_ref u), ``sipg.py:565,597,853``; with ``cub`` the cubature
+    mass ``cubature_mass_apply`` (``cubature.py:243-254``)."""
+    if cub is not None:
+        from .cubature import cubature_mass_apply
+        return cubature_mass_apply(cub, u)
     if u.ndim == 3:
         return mesh.J[:, :, None] * np.einsum("ij,jkb->ikb", mesh.ref.M, u)
     return mesh.J * (mesh.ref.M @ u)
 
 
-def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, kappa=None):
+def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, kappa=None, cub=None):
     """Matvec on the element-major flat vector; ``alpha M + A`` (alpha=0:
     ``sipg.py:876-883``; alpha>0: ``sipg.py:589-601`` and
     ``multigrid.py:53-74``).  Accepts (n,) or (n, B)."""
@@ -264,19 +321,19 @@ def flat_op(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, kappa=None):
     def op(x):
         X = x[:, None] if x.ndim == 1 else x
         U = _unflat(X, Np, K)
-        Y = apply(mesh, U, bc_types=bc_types, tau_scale=tau_scale, kappa=kappa)
+        Y = apply(mesh, U, bc_types=bc_types, tau_scale=tau_scale, kappa=kappa, cub=cub)
         if alpha != 0.0:
-            Y = Y + alpha * mass_apply(mesh, U)
+            Y = Y + alpha * mass_apply(mesh, U, cub)
         out = _flat(Y)
         return out[:, 0] if x.ndim == 1 else out
     return op
 
 
-def dense_matrix(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, chunk=512, kappa=None):
+def dense_matrix(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, chunk=512, kappa=None, cub=None):
     """``sipg_matrix_2d`` (``sipg.py:344-364``) / ``sipg_helmholtz_matrix_2d``
     (``:460-496``; ``nu`` unused there too): columns of the apply."""
     n = mesh.Np * mesh.K
-    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha, kappa=kappa)
+    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha, kappa=kappa, cub=cub)
     A = np.zeros((n, n))
     for c0 in range(0, n, chunk):
         c1 = min(n, c0 + chunk)
@@ -399,8 +456,10 @@ def make_block_jacobi(mesh, *, bc_types, tau_scale=200.0, alpha=0.0, matfree=Tru
 
 # ------------------------------------------------------------ solves ------
 
-def _rhs(mesh, source, bc_types, u_dir, q_neu, tau_scale):
-    rhs = mass_apply(mesh, np.asarray(source, dtype=np.float64))
+def _rhs(mesh, source, bc_types, u_dir, q_neu, tau_scale, cub=None):
+    # the mass of the source uses the cubature; the Dirichlet load does not
+    # (sipg.py:852-864, :404-417)
+    rhs = mass_apply(mesh, np.asarray(source, dtype=np.float64), cub)
     if u_dir is not None:
         rhs = rhs - dirichlet_load(mesh, np.asarray(u_dir, dtype=np.float64),
                                    bc_types=bc_types, tau_scale=tau_scale)
@@ -410,16 +469,16 @@ def _rhs(mesh, source, bc_types, u_dir, q_neu, tau_scale):
 
 
 def solve_poisson(mesh, source, *, bc_types, u_dir=None, q_neu=None, tau_scale=200.0,
-                  iterative=None, x0=None, preconditioner=None, return_info=False):
+                  iterative=None, x0=None, preconditioner=None, return_info=False, cub=None):
     """``solve_sipg_poisson_2d`` (``sipg.py:812-918``)."""
     import scipy.linalg as sla
     Np, K = mesh.Np, mesh.K
-    b = _rhs(mesh, source, bc_types, u_dir, q_neu, tau_scale)
+    b = _rhs(mesh, source, bc_types, u_dir, q_neu, tau_scale, cub)
     if iterative is None:
-        A = dense_matrix(mesh, bc_types=bc_types, tau_scale=tau_scale)
+        A = dense_matrix(mesh, bc_types=bc_types, tau_scale=tau_scale, cub=cub)
         x = sla.lu_solve(sla.lu_factor(A), b)
         return x.reshape(K, Np).T
-    raw = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale)
+    raw = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, cub=cub)
     singular = not bool(np.any(np.asarray(bc_types) == BC_DIRICHLET))
     if singular:                                                     # :891-906
         probe = np.sin(np.arange(Np * K, dtype=np.float64))
@@ -440,18 +499,18 @@ def solve_poisson(mesh, source, *, bc_types, u_dir=None, q_neu=None, tau_scale=2
 
 def solve_helmholtz(mesh, rhs_field, *, alpha, nu=1.0, bc_types, u_dir=None, q_neu=None,
                     tau_scale=200.0, iterative=None, x0=None, preconditioner=None,
-                    return_info=False):
+                    return_info=False, cub=None):
     """``solve_sipg_helmholtz_2d`` (``sipg.py:536-612``); ``nu`` is unused,
     as in the reference."""
     import scipy.linalg as sla
     Np, K = mesh.Np, mesh.K
-    b = _rhs(mesh, rhs_field, bc_types, u_dir, q_neu, tau_scale)
+    b = _rhs(mesh, rhs_field, bc_types, u_dir, q_neu, tau_scale, cub)
     if iterative is None:
-        A = dense_matrix(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha)
+        A = dense_matrix(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha, cub=cub)
         return sla.lu_solve(sla.lu_factor(A), b).reshape(K, Np).T
     if iterative.method != "cg":
         raise ValueError(f"iterative method {iterative.method!r} not supported for SPD")
-    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha)
+    op = flat_op(mesh, bc_types=bc_types, tau_scale=tau_scale, alpha=alpha, cub=cub)
     xf = None if x0 is None else np.asarray(x0).T.reshape(-1)
     x, it = cg(op, b, xf, tol=iterative.tol, atol=iterative.atol,
                maxiter=iterative.maxiter, M=preconditioner)

@@ -34,8 +34,17 @@ here is computed by the reference's code path:
   the reference test's channel, by direct LU and by multigrid-preconditioned
   CG, and a second (BDF2) step.
 
+* curved elements (``curved.npz``, also alone with ``--only curved``): the
+  hole-bounded builders ``rectangle_with_square_hole_mesh_2d`` and
+  ``channel_with_circle_mesh_2d``, the boundary bending of
+  ``apply_circular_hole_2d``, ``attach_cubature``, ``per_element_mass``,
+  ``cubature_mass_apply``, ``sipg_apply_2d`` with and without ``cub`` on the
+  curved meshes, the loads there, block diagonals by coloured probing, and
+  ``solve_sipg_poisson_2d`` / ``solve_sipg_helmholtz_2d`` with ``cub`` by LU
+  and CG.
+
 Outputs: ``refelem.npz``, ``meshes.npz``, ``applies.npz``, ``solves.npz``,
-``ins.npz`` next to this file.
+``ins.npz``, ``curved.npz`` next to this file.
 """
 
 from __future__ import annotations
@@ -77,8 +86,116 @@ def bc_sets(m, rng):
     }
 
 
-def main(src: str) -> None:
+CUB_FIELDS = ("r", "s", "w", "Lq", "Drq", "Dsq", "J", "rx", "sx", "ry", "sy", "face_w", "face_Lq",
+              "face_L1d", "face_sJ", "face_nx", "face_ny")
+
+
+def curved_fixtures(imp) -> dict:
+    """Fixtures of the curved-element (cubature) branch."""
+    rmesh = imp("ddg.dg2d.mesh")
+    rsipg = imp("ddg.dg2d.sipg")
+    rcur = imp("ddg.dg2d.curved")
+    rcub = imp("ddg.dg2d.cubature")
+    IC = rsipg.IterativeConfig
+    out = {}
+    t0 = time.time()
+    rng = np.random.default_rng(31)
+    # the reference test's annulus (square hole bent onto its inscribed
+    # circle), coarser, and a cylinder-in-channel O-grid mesh
+    VX, VY, E = rmesh.rectangle_with_square_hole_mesh_2d(-2.0, 2.0, -2.0, 2.0, 8, 8, -0.5, 0.5, -0.5, 0.5)
+    base = rmesh.build_mesh_2d(VX, VY, E, 3)
+    ann = rcur.apply_circular_hole_2d(base, cx=0.0, cy=0.0, radius=0.5, detection_tol=0.5)
+    VX2, VY2, E2 = rmesh.channel_with_circle_mesh_2d(0.0, 2.0, 0.0, 2.0, 8, 8, cx=1.0, cy=1.0, radius=0.25,
+                                                     R_outer=0.5, n_radial=3, radial_growth=1.3)
+    base2 = rmesh.build_mesh_2d(VX2, VY2, E2, 4)
+    cyl = rcur.apply_circular_hole_2d(base2, cx=1.0, cy=1.0, radius=0.25, detection_tol=0.1)
+    meshes = {"annulus8_N3": (ann, (VX, VY, E)), "cyl8_N4": (cyl, (VX2, VY2, E2))}
+    cubs = {}
+    for name, (m, (vx, vy, ee)) in meshes.items():
+        out[f"{name}/VX"], out[f"{name}/VY"], out[f"{name}/EToV"] = _a(vx), _a(vy), _a(ee)
+        for f in MESH_FIELDS:
+            out[f"{name}/mesh/{f}"] = _a(getattr(m, f))
+        out[f"{name}/N"] = np.int64(m.N)
+        cub = rcub.attach_cubature(m)
+        cubs[name] = cub
+        for f in CUB_FIELDS:
+            out[f"{name}/cub/{f}"] = _a(getattr(cub, f))
+        K, Np = int(m.K), int(m.Np)
+        fld = rng.standard_normal((Np, K))
+        out[f"{name}/mass/f"] = fld
+        out[f"{name}/mass/Mf"] = _a(rcub.cubature_mass_apply(cub, fld))
+        if name == "annulus8_N3":
+            out[f"{name}/mass/MK"] = _a(rcub.per_element_mass(cub))
+        sets = bc_sets(m, rng)
+        for bname in ("dirichlet", "random", "neumann"):
+            for tau in (200.0, 0.5):
+                bc = sets[bname]
+                u = rng.standard_normal((Np, K))
+                key = f"{name}/apply/{bname}/tau{tau:g}"
+                out[key + "/bc"] = bc
+                out[key + "/u"] = u
+                out[key + "/Au_nodal"] = _a(rsipg.sipg_apply_2d(m, u, bc_types=bc, tau_scale=tau))
+                out[key + "/Au_cub"] = _a(rsipg.sipg_apply_2d(m, u, bc_types=bc, tau_scale=tau, cub=cub))
+        bc = sets["random"]
+        u = rng.standard_normal((Np, K))
+        ud = np.sin(1.3 * _a(m.x)) * np.cos(0.7 * _a(m.y))
+        q = rng.standard_normal((3 * int(m.Nfp), K))
+        out[f"{name}/udir/bc"] = bc
+        out[f"{name}/udir/u"] = u
+        out[f"{name}/udir/u_dir"] = ud
+        out[f"{name}/udir/q_neu"] = q
+        out[f"{name}/udir/Au_cub"] = _a(rsipg.sipg_apply_2d(m, u, bc_types=bc, u_dir=ud, tau_scale=200.0, cub=cub))
+        out[f"{name}/udir/LD"] = _a(rsipg.sipg_dirichlet_load_2d(m, ud, bc_types=bc, tau_scale=200.0))
+        out[f"{name}/udir/LN"] = _a(rsipg.sipg_neumann_load_2d(m, q, bc_types=bc))
+        print(f"curved {name} applies {time.time() - t0:.1f}s", flush=True)
+
+    # block diagonals (coloured probing) of the nodal and the cubature operator
+    m = ann
+    cub = cubs["annulus8_N3"]
+    bc = bc_sets(m, rng)["dirichlet"]
+    K, Np = int(m.K), int(m.Np)
+    for tag, c in (("nodal", None), ("cub", cub)):
+        def apply_flat(v, c=c):
+            return rsipg.sipg_apply_2d(m, v.reshape(K, Np).T, bc_types=bc, tau_scale=200.0, cub=c).T.reshape(-1)
+        out[f"annulus8_N3/blocks/{tag}"] = _a(rsipg.extract_block_diag_matfree(apply_flat, m))
+    out["annulus8_N3/blocks/bc"] = bc
+
+    # the reference test's manufactured Poisson solve, all-Dirichlet, with and
+    # without cubature, by LU; with cubature also by CG
+    ue = np.sin(np.pi * _a(m.x) / 4) * np.sin(np.pi * _a(m.y) / 4)
+    src = 2 * (np.pi / 4) ** 2 * ue
+    out["annulus8_N3/solve/bc"] = bc
+    out["annulus8_N3/solve/u_exact"] = ue
+    out["annulus8_N3/solve/u_lu_nodal"] = _a(rsipg.solve_sipg_poisson_2d(m, src, bc_types=bc, u_dir=ue))
+    out["annulus8_N3/solve/u_lu_cub"] = _a(rsipg.solve_sipg_poisson_2d(m, src, bc_types=bc, u_dir=ue, cub=cub))
+    x = rsipg.solve_sipg_poisson_2d(m, src, bc_types=bc, u_dir=ue, cub=cub, iterative=IC(tol=1e-10, maxiter=5000))
+    out["annulus8_N3/solve/u_cg_cub"] = _a(x)
+    out["annulus8_N3/solve/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    print(f"curved poisson CG {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+    # Helmholtz with cubature (mass by cubature), mixed BCs, CG and LU
+    m = cyl
+    cub = cubs["cyl8_N4"]
+    bc = bc_sets(m, rng)["random"]
+    rhs = np.cos(2.0 * _a(m.x)) * np.sin(1.5 * _a(m.y)) + 0.2
+    out["cyl8_N4/helm/bc"] = bc
+    out["cyl8_N4/helm/rhs"] = rhs
+    x = rsipg.solve_sipg_helmholtz_2d(m, rhs, alpha=5.0, nu=1.0, bc_types=bc, tau_scale=0.5, cub=cub,
+                                      iterative=IC(tol=1e-10, maxiter=8000))
+    out["cyl8_N4/helm/u_cg"] = _a(x)
+    out["cyl8_N4/helm/cg_iterations"] = np.int64(refshim.cg_last_iterations())
+    print(f"curved helmholtz CG {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
+    out["cyl8_N4/helm/u_lu"] = _a(rsipg.solve_sipg_helmholtz_2d(m, rhs, alpha=5.0, nu=1.0, bc_types=bc,
+                                                                 tau_scale=0.5, cub=cub))
+    print(f"curved done {time.time() - t0:.1f}s", flush=True)
+    return out
+
+
+def main(src: str, only: str | None = None) -> None:
     imp = refshim.install(src)
+    if only == "curved":
+        d = curved_fixtures(imp)
+        np.savez_compressed(os.path.join(HERE, "curved.npz"), **{k: np.asarray(v) for k, v in d.items()})
+        return
     rmesh = imp("ddg.dg2d.mesh")
     rsipg = imp("ddg.dg2d.sipg")
     rmg = imp("ddg.dg2d.multigrid")
@@ -298,11 +415,14 @@ def main(src: str) -> None:
             out_ins[f"{tag}/{name}"] = _a(v)
     print(f"ins done {time.time() - t0:.1f}s", flush=True)
 
+    out_cur = curved_fixtures(imp)
     for fname, d in (("refelem.npz", out_ref), ("meshes.npz", out_mesh), ("applies.npz", out_app),
-                     ("solves.npz", out_sol), ("ins.npz", out_ins)):
+                     ("solves.npz", out_sol), ("ins.npz", out_ins), ("curved.npz", out_cur)):
         np.savez_compressed(os.path.join(HERE, fname), **{k: np.asarray(v) for k, v in d.items()})
     print(f"wrote fixtures in {time.time() - t0:.1f}s")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    args = [a for a in sys.argv[1:] if not a.startswith("--only")]
+    only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
+    main(args[0] if args else "/root/reference/src", only)
