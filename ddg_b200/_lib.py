@@ -20,6 +20,8 @@ DDG_PC_JACOBI = 1
 DDG_MAX_DEGREE = 5
 DDG_ENGINE_CUDA_CORES = 0
 DDG_ENGINE_TENSOR_CORES = 1
+DDG_QUAD_NODAL = 0
+DDG_QUAD_CUBATURE = 1
 SOLVE_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "device_error", 4: "stagnated"}
 
 
@@ -41,6 +43,23 @@ class MeshDesc(C.Structure):
                 ("EToE", C.POINTER(C.c_int64)), ("EToF", C.POINTER(C.c_int64)),
                 ("vmapM", C.POINTER(C.c_int64)), ("vmapP", C.POINTER(C.c_int64)),
                 ("bc_types", C.POINTER(C.c_int32))]
+
+
+_dp = C.POINTER(C.c_double)
+
+
+class CurvedDesc(C.Structure):
+    _fields_ = [("N", C.c_int32), ("K", C.c_int32), ("device", C.c_int32), ("Ncub", C.c_int32),
+                ("Nfq", C.c_int32), ("reserved", C.c_int32), ("tau_scale", C.c_double),
+                ("Dr", _dp), ("Ds", _dp), ("M", _dp), ("m1d", _dp), ("Fmask", C.POINTER(C.c_int64)),
+                ("rx", _dp), ("sx", _dp), ("ry", _dp), ("sy", _dp), ("J", _dp),
+                ("nx", _dp), ("ny", _dp), ("sJ", _dp), ("Fscale", _dp),
+                ("EToE", C.POINTER(C.c_int64)), ("EToF", C.POINTER(C.c_int64)),
+                ("vmapM", C.POINTER(C.c_int64)), ("vmapP", C.POINTER(C.c_int64)),
+                ("bc_types", C.POINTER(C.c_int32)),
+                ("cw", _dp), ("Drq", _dp), ("Dsq", _dp), ("Lq", _dp),
+                ("cJ", _dp), ("crx", _dp), ("csx", _dp), ("cry", _dp), ("csy", _dp),
+                ("face_w", _dp), ("face_L1d", _dp), ("face_sJ", _dp)]
 
 
 class CgConfig(C.Structure):
@@ -93,6 +112,17 @@ _PROTOS = {
     "ddg_pool_poll": (C.c_int, [_vp, _vp, _vp, _vp]),
     "ddg_pool_retire": (C.c_int, [_vp, C.c_int, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_sipg_upload_reference": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, C.c_int]),
+    "ddg_curved_create": (C.c_int, [C.POINTER(CurvedDesc), C.POINTER(_vp)]),
+    "ddg_curved_destroy": (C.c_int, [_vp]),
+    "ddg_curved_set_bc": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
+    "ddg_curved_apply": (C.c_int, [_vp, C.c_int, C.c_double, _vp, _vp, _vp]),
+    "ddg_curved_apply_dir": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
+    "ddg_curved_mass": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "ddg_curved_rhs": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "ddg_curved_pc_build": (C.c_int, [_vp, C.c_int, C.c_double, _vp]),
+    "ddg_curved_pc_apply": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ddg_curved_pc_blocks": (C.c_int, [_vp, _vp, _vp]),
+    "ddg_curved_cg": (C.c_int, [_vp, C.c_int, C.POINTER(CgConfig), _vp, _vp, _vp, C.POINTER(SolveInfo)]),
     "ddg_sipg_set_kappa": (C.c_int, [_vp, _vp]),
     "ddg_sipg_grad_kappa": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "ddg_axpby": (C.c_int, [_i64, C.c_double, _vp, C.c_double, _vp, _vp]),

@@ -52,6 +52,8 @@ class _KappaState:
 
 
 def _state(op):
+    if not isinstance(op, SipgOperator):
+        raise ValueError("the per-element diffusivity (kappa) is built for straight-sided (affine) meshes only")
     s = getattr(op, "_kappa_state", None)
     if s is None:
         s = op._kappa_state = _KappaState()

@@ -17,7 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libddg_sipg.so")
 
-CU_SOURCES = ["sipg_kernels.cu", "sipg_mg.cu", "sipg_capi.cu", "sipg_pool.cu", "noalloc.cu"]
+CU_SOURCES = ["sipg_kernels.cu", "sipg_curved.cu", "sipg_mg.cu", "sipg_capi.cu", "sipg_curved_capi.cu",
+              "sipg_pool.cu", "noalloc.cu"]
 CXX_SOURCES = ["mesh_connect.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -48,19 +49,36 @@ def up_to_date() -> bool:
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every translation unit to an object (in parallel: the kernel
+    units take minutes each), then link the shared library."""
     if not force and up_to_date():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O2",
-           "--expt-relaxed-constexpr", "-o", LIB + ".tmp", *_sources()]
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        r = subprocess.run([_nvcc(), *flags, "-c", src, "-o", obj], capture_output=True, text=True)
+        return src, obj, r
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        results = list(ex.map(compile_one, _sources()))
+    for src, _, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    r = subprocess.run([_nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *[o for _, o, _ in results]],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libddg_sipg.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libddg_sipg.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

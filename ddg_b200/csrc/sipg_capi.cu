@@ -446,6 +446,7 @@ extern "C" int ddg_sipg_upload_reference(int N, const double* Dr, const double* 
     cudaGetDevice(&cur);
     cudaSetDevice(device);
     cudaError_t e = upload_ref(N, Dr, Ds, M, m1d);
+    if (e == cudaSuccess) e = cv_upload_ref(N, Dr, Ds, M, m1d);
     cudaSetDevice(cur);
     if (e != cudaSuccess) return fail(DDG_ERR_CUDA, std::string("constant upload: ") + cudaGetErrorString(e));
     g_ref_loaded[key] = blob;

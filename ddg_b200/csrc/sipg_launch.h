@@ -128,6 +128,48 @@ struct RhsArgs {
   double tau;
 };
 
+// Curved-element operator (per-node geometric factors, nodal or cubature
+// quadrature): every per-element field is [field][row][K].
+struct CvArgs {
+  int K;               // elements (the SoA stride of every field)
+  int Ncub;            // volume cubature points (cubature quadrature)
+  const double* gN;    // [5][Np][K] rx sx ry sy J at the nodes
+  const double* fN;    // [2][3Nfp][K] nx ny at the face nodes
+  const double* sJ0;   // [3][K] sJ at each face's first node
+  const double* tauF;  // [3][K] tau_scale (N+1)^2 Fscale at each face's first node
+  const int* tag;      // [3][K] BC tag of (k, f)
+  const int* slotP;    // [3Nfp][K] vmapP: element-major index of the outside trace node
+  const int* mapP;     // [3Nfp][K] the matching face slot of the neighbour, m' K + k'
+  const double* cG;    // [4][Ncub][K] wJ(rx^2+ry^2), wJ(rx sx+ry sy), wJ(sx^2+sy^2), wJ
+  const double* cQ;    // [3][Nfp(Nfp+1)/2][K] packed face rule L1d^T diag(face_w sJ) L1d
+  const double* cMat;  // [3][Ncub][Np] Drq, Dsq, Lq
+  double* tr;          // [2][3Nfp][K] gradient traces (pass 1)
+  double* dl;          // [3][3Nfp][K] face duals (pass 2)
+  CgCtl* ctl;          // CG control block (PDOT, RESID; gating inside CG graphs)
+  double* partA;       // per-block partials
+  double* partB;
+  int gate;            // skip the launch once ctl->cont == 0 (CG graph bodies)
+};
+// dynamic shared memory ceiling of the curved kernels (bytes)
+#define CV_SMEM_LIMIT (200 * 1024)
+// pass 1 (traces of u), 2 (face duals, udir = Dirichlet data or null),
+// 3 (gather: mode 0 y = A u + alpha M u + shift u, 1 y -= that, 2 with the
+// p.Ap reduction, 3 y = b - that with b.b and r.r); quad 1 = cubature
+cudaError_t launch_cv_pass(int N, int pass, int quad, int mode, const CvArgs& a, const double* u, const double* udir,
+                           const double* b, double* y, double alpha, double shift, cudaStream_t s);
+cudaError_t cv_prepare(int N);
+// the curved kernels' copy of the reference-element matrices
+cudaError_t cv_upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d);
+cudaError_t launch_cv_mass(int N, int quad, const CvArgs& a, const double* f, double* y, cudaStream_t s);
+cudaError_t launch_cv_neumann(int N, const CvArgs& a, const double* q, double* y, cudaStream_t s);
+cudaError_t launch_cv_probe(int K, int Np, const int* colour, int c, int j, double* P, cudaStream_t s);
+cudaError_t launch_cv_collect(int K, int Np, const int* colour, int c, int j, double shift, const double* Y,
+                              double* blocks, cudaStream_t s);
+cudaError_t launch_cv_invert(int N, int K, const double* blocks, double* binv, unsigned int* status, cudaStream_t s);
+cudaError_t launch_cv_pc(int N, int K, const double* binv, const double* r, double* z, const CgCtl* ctl,
+                         cudaStream_t s);
+cudaError_t launch_cv_pupd(int64_t n, const double* z, double* p, const CgCtl* ctl, cudaStream_t s);
+
 cudaError_t upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d);
 template <typename T>
 cudaError_t launch_apply(int N, int mode, const ApplyArgs<T>& a, cudaStream_t s);

@@ -1,7 +1,9 @@
 """2D triangle mesh (host setup) with the field names of ddg's ``Mesh2D``.
 
-Mirrors ``src/ddg/dg2d/mesh.py``: ``uniform_rectangle_mesh_2d`` (:125-156)
-and ``build_mesh_2d`` (:691-760) produce the same arrays (volume fields
+Mirrors ``src/ddg/dg2d/mesh.py``: ``uniform_rectangle_mesh_2d`` (:125-156),
+the hole-bounded builders ``rectangle_with_square_hole_mesh_2d`` (:159-212)
+and ``channel_with_circle_mesh_2d`` (:307-513), and ``build_mesh_2d``
+(:691-760) produce the same arrays (volume fields
 ``(Np, K)``, face fields ``(3 Nfp, K)``, ``vmapM``/``vmapP`` into the
 element-major flat vector).  The topological connectivity (``EToE``,
 ``EToF``) and the node maps are computed by the C++ routines
@@ -38,6 +40,97 @@ def uniform_rectangle_mesh_2d(xmin, xmax, ymin, ymax, Kx: int, Ky: int):
     upper = np.stack([v00, v11, v01], axis=1)
     EToV = np.stack([lower, upper], axis=1).reshape(-1, 3).astype(np.int64)
     return VX, VY, EToV
+
+
+def _prune(VX, VY, EToV):
+    """Drop unused vertices and renumber (``mesh.py:205-212``)."""
+    used = np.unique(EToV.reshape(-1))
+    remap = -np.ones(VX.shape[0], dtype=np.int64)
+    remap[used] = np.arange(used.shape[0])
+    return VX[used], VY[used], remap[EToV]
+
+
+def _cell_triangles(Kx: int, keep: np.ndarray) -> np.ndarray:
+    """The two triangles of every kept cell (j, i) of the structured split,
+    in row-major cell order (``mesh.py:125-156``)."""
+    j, i = np.nonzero(keep)
+    v00 = j * (Kx + 1) + i
+    v10, v01 = v00 + 1, v00 + Kx + 1
+    v11 = v01 + 1
+    lower = np.stack([v00, v10, v11], axis=1)
+    upper = np.stack([v00, v11, v01], axis=1)
+    return np.stack([lower, upper], axis=1).reshape(-1, 3).astype(np.int64)
+
+
+def rectangle_with_square_hole_mesh_2d(xmin, xmax, ymin, ymax, Kx: int, Ky: int,
+                                       hole_xmin, hole_xmax, hole_ymin, hole_ymax):
+    """The uniform split without the cells whose centre lies in the hole box,
+    unused vertices pruned (``src/ddg/dg2d/mesh.py:159-212``)."""
+    xs = np.linspace(xmin, xmax, Kx + 1)
+    ys = np.linspace(ymin, ymax, Ky + 1)
+    cx = 0.5 * (xs[:-1] + xs[1:])
+    cy = 0.5 * (ys[:-1] + ys[1:])
+    inside = ((hole_xmin <= cx[None, :]) & (cx[None, :] <= hole_xmax)
+              & (hole_ymin <= cy[:, None]) & (cy[:, None] <= hole_ymax))
+    E = _cell_triangles(Kx, ~inside)
+    return _prune(np.tile(xs, Ky + 1), np.repeat(ys, Kx + 1), E)
+
+
+def channel_with_circle_mesh_2d(xmin, xmax, ymin, ymax, Kx: int, Ky: int, *, cx, cy, radius, R_outer,
+                                n_radial: int = 4, radial_growth: float = 1.0):
+    """Channel with a circular hole, body-fitted by an O-grid
+    (``src/ddg/dg2d/mesh.py:307-513``): the Cartesian split minus the
+    grid-aligned bounding square of half-side ``R_outer``, plus
+    ``n_radial`` layers of wedges between the square's perimeter and the
+    polygonal cylinder (inner vertices at the perimeter vertices' angles).
+    Call ``curved.apply_circular_hole_2d`` to bend the inner faces."""
+    if not radius < R_outer:
+        raise ValueError(f"radius={radius} must be < R_outer={R_outer}")
+    if not (cx - R_outer > xmin and cx + R_outer < xmax and cy - R_outer > ymin and cy + R_outer < ymax):
+        raise ValueError("Bounding square must lie strictly inside the channel")
+    hx, hy = (xmax - xmin) / Kx, (ymax - ymin) / Ky
+    idx = {}
+    for name, v in (("i_lo", (cx - R_outer - xmin) / hx), ("i_hi", (cx + R_outer - xmin) / hx),
+                    ("j_lo", (cy - R_outer - ymin) / hy), ("j_hi", (cy + R_outer - ymin) / hy)):
+        if abs(v - round(v)) > 1e-9:
+            raise ValueError(f"Bounding square not grid-aligned: {name}={v} (must be integral)")
+        idx[name] = int(round(v))
+    i_lo, i_hi, j_lo, j_hi = idx["i_lo"], idx["i_hi"], idx["j_lo"], idx["j_hi"]
+    xs = np.linspace(xmin, xmax, Kx + 1)
+    ys = np.linspace(ymin, ymax, Ky + 1)
+    VXf, VYf = np.tile(xs, Ky + 1), np.repeat(ys, Kx + 1)
+    jj, ii = np.meshgrid(np.arange(Ky), np.arange(Kx), indexing="ij")
+    E_outer = _cell_triangles(Kx, ~((i_lo <= ii) & (ii < i_hi) & (j_lo <= jj) & (jj < j_hi)))
+    vid = lambda i, j: j * (Kx + 1) + i  # noqa: E731
+    # perimeter of the square, counter-clockwise from its bottom-left corner (mesh.py:280-304)
+    outer = np.concatenate([vid(np.arange(i_lo, i_hi), j_lo), vid(i_hi, np.arange(j_lo, j_hi)),
+                            vid(np.arange(i_hi, i_lo, -1), j_hi), vid(i_lo, np.arange(j_hi, j_lo, -1))]
+                           ).astype(np.int64)
+    nc = outer.shape[0]
+    if nc < 8:
+        raise ValueError(f"Bounding square has only {nc} perimeter vertices; need at least 8")
+    OX, OY = VXf[outer], VYf[outer]
+    th = np.arctan2(OY - cy, OX - cx)
+    IX, IY = cx + radius * np.cos(th), cy + radius * np.sin(th)
+    if abs(radial_growth - 1.0) < 1e-12:
+        frac = np.linspace(0.0, 1.0, n_radial + 1)
+    else:
+        g = radial_growth
+        w0 = 1.0 / ((g ** n_radial - 1.0) / (g - 1.0))
+        frac = np.concatenate(([0.0], np.cumsum(w0 * g ** np.arange(n_radial))))
+    n0 = VXf.shape[0]
+    layers = [n0 + L * nc + np.arange(nc, dtype=np.int64) for L in range(n_radial)] + [outer]
+    LX = [IX + frac[L] * (OX - IX) for L in range(n_radial)]
+    LY = [IY + frac[L] * (OY - IY) for L in range(n_radial)]
+    i = np.arange(nc)
+    ip = (i + 1) % nc
+    wedge = []
+    for L in range(n_radial):
+        A, B = layers[L][i], layers[L][ip]
+        C, D = layers[L + 1][ip], layers[L + 1][i]
+        wedge.append(np.stack([np.stack([A, D, C], 1), np.stack([A, C, B], 1)], 1).reshape(-1, 3))
+    E = np.concatenate([E_outer] + wedge)
+    return _prune(np.concatenate([VXf] + LX), np.concatenate([VYf] + LY), E)
 
 
 @dataclass(eq=False)
@@ -77,11 +170,32 @@ class Mesh2D:
     vmapP: np.ndarray
     vmapB: np.ndarray
     mapB: np.ndarray
-    _ops: dict = field(default_factory=dict, repr=False)
+    # device operators built on this mesh (not copied by dataclasses.replace)
+    _ops: dict = field(default_factory=dict, init=False, repr=False, compare=False)
+    _affine: object = field(default=None, init=False, repr=False, compare=False)
 
     @property
     def ref(self) -> RefElement:
         return ref_element(self.N)
+
+    @property
+    def is_affine(self) -> bool:
+        """True when every element is a straight-sided triangle: the
+        geometric factors are constant over each element (to 1e-10 of their
+        magnitude) and so are the normals and sJ of each face.  Curved
+        meshes (``curved.project_to_curve_2d``) are not."""
+        if self._affine is None:
+            def const(a, rows):
+                a = np.asarray(a)
+                ref = a[rows]
+                scale = max(float(np.max(np.abs(a))), 1e-300)
+                return float(np.max(np.abs(a - ref))) <= 1e-10 * scale
+            Nfp = self.Nfp
+            first = np.repeat(np.arange(3) * Nfp, Nfp)
+            ok = all(const(a, np.zeros(self.Np, dtype=np.int64)) for a in (self.rx, self.sx, self.ry, self.sy, self.J))
+            ok = ok and all(const(a, first) for a in (self.nx, self.ny, self.sJ, self.Fscale))
+            object.__setattr__(self, "_affine", bool(ok))
+        return self._affine
 
     def element_geometry(self) -> np.ndarray:
         """(K, 14) per-element affine geometry: rx sx ry sy J, then nx ny sJ
@@ -100,7 +214,11 @@ class Mesh2D:
 
     def device_operator(self, bc_types, tau_scale: float = 200.0, device: int | None = None):
         """The device-resident SIPG operator for these BC tags and penalty,
-        cached per (tau_scale, device, BC tags); a few BC sets are kept."""
+        cached per (tau_scale, device, BC tags); a few BC sets are kept.
+        A curved mesh gets the curved-element operator with the nodal
+        quadrature (the reference's ``cub=None`` on such a mesh)."""
+        if not self.is_affine:
+            return self.curved_operator(bc_types, tau_scale, None, device)
         from .operator import SipgOperator
         import torch
         dev = torch.cuda.current_device() if device is None else int(device)
@@ -117,6 +235,27 @@ class Mesh2D:
                 # last reference
                 self._ops.pop(next(iter(self._ops)))
         self._ops[key] = op            # most recently used last
+        return op
+
+    def curved_operator(self, bc_types, tau_scale: float = 200.0, cub=None, device: int | None = None):
+        """The curved-element operator (per-node geometric factors; nodal
+        quadrature, plus the cubature rule of ``cub`` when given), cached per
+        (tau_scale, device, BC tags, cub) like :meth:`device_operator`."""
+        from .curved_operator import CurvedOperator
+        import torch
+        dev = torch.cuda.current_device() if device is None else int(device)
+        bc = np.ascontiguousarray(np.asarray(bc_types), dtype=np.int32)
+        if bc.shape != (self.K, 3):
+            raise ValueError(f"bc_types must have shape (K, 3) = ({self.K}, 3), got {bc.shape}")
+        if cub is not None and cub.mesh is not self:
+            raise ValueError("cub was attached to a different mesh")
+        key = ("curved", float(tau_scale), dev, bc.tobytes(), id(cub) if cub is not None else None)
+        op = self._ops.pop(key, None)
+        if op is None or op.cub is not cub:
+            op = CurvedOperator(self, bc, tau_scale=tau_scale, cub=cub, device=dev)
+            while len(self._ops) >= 4:
+                self._ops.pop(next(iter(self._ops)))
+        self._ops[key] = op
         return op
 
 
@@ -143,18 +282,11 @@ def _maps(N, Fmask, x, y, EToE, EToF, EToV, VX, VY, node_tol=1e-10):
     return vmapM, vmapP
 
 
-def build_mesh_2d(VX, VY, EToV, N: int) -> Mesh2D:
-    """StartUp2D: ``src/ddg/dg2d/mesh.py:691-760``."""
-    EToV = np.asarray(EToV, dtype=np.int64)
-    VX = np.asarray(VX, dtype=np.float64)
-    VY = np.asarray(VY, dtype=np.float64)
-    K = EToV.shape[0]
-    ref = ref_element(N)
-    Np, Nfp = ref.Np, ref.Nfp
-    r, s = ref.r, ref.s
-    va, vb, vc = EToV[:, 0], EToV[:, 1], EToV[:, 2]
-    x = 0.5 * (np.outer(-(r + s), VX[va]) + np.outer(1.0 + r, VX[vb]) + np.outer(1.0 + s, VX[vc]))
-    y = 0.5 * (np.outer(-(r + s), VY[va]) + np.outer(1.0 + r, VY[vb]) + np.outer(1.0 + s, VY[vc]))
+def geometry_2d(ref: RefElement, x, y):
+    """Geometric factors at the nodes and face normals of elements with node
+    coordinates (x, y) (``src/ddg/dg2d/mesh.py:634-684``): returns
+    rx, sx, ry, sy, J (Np, K) and nx, ny, sJ, Fscale (3 Nfp, K)."""
+    Nfp, K = ref.Nfp, x.shape[1]
     xr, xs, yr, ys = ref.Dr @ x, ref.Ds @ x, ref.Dr @ y, ref.Ds @ y
     J = xr * ys - xs * yr
     rx, sx, ry, sy = ys / J, -yr / J, -xs / J, xr / J
@@ -169,6 +301,22 @@ def build_mesh_2d(VX, VY, EToV, N: int) -> Mesh2D:
     sJ = np.sqrt(nx * nx + ny * ny)
     nx, ny = nx / sJ, ny / sJ
     Fscale = sJ / J[ff, :]
+    return rx, sx, ry, sy, J, nx, ny, sJ, Fscale
+
+
+def build_mesh_2d(VX, VY, EToV, N: int) -> Mesh2D:
+    """StartUp2D: ``src/ddg/dg2d/mesh.py:691-760``."""
+    EToV = np.asarray(EToV, dtype=np.int64)
+    VX = np.asarray(VX, dtype=np.float64)
+    VY = np.asarray(VY, dtype=np.float64)
+    K = EToV.shape[0]
+    ref = ref_element(N)
+    Np, Nfp = ref.Np, ref.Nfp
+    r, s = ref.r, ref.s
+    va, vb, vc = EToV[:, 0], EToV[:, 1], EToV[:, 2]
+    x = 0.5 * (np.outer(-(r + s), VX[va]) + np.outer(1.0 + r, VX[vb]) + np.outer(1.0 + s, VX[vc]))
+    y = 0.5 * (np.outer(-(r + s), VY[va]) + np.outer(1.0 + r, VY[vb]) + np.outer(1.0 + s, VY[vc]))
+    rx, sx, ry, sy, J, nx, ny, sJ, Fscale = geometry_2d(ref, x, y)
     EToE, EToF = _connect(EToV)
     vmapM, vmapP = _maps(N, ref.Fmask, x, y, EToE, EToF, EToV, VX, VY)
     mapB = np.flatnonzero(vmapP == vmapM)

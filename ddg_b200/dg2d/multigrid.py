@@ -73,6 +73,9 @@ class SipgMultigrid:
         self.alpha = float(alpha)
         self.tau_scale = float(tau_scale)
         self.meshes = meshes
+        if not all(m.is_affine for m in meshes):
+            raise ValueError("the device multigrid needs straight-sided (affine) levels; use block-Jacobi "
+                             "or no preconditioner on curved meshes")
         self.ops = [m.device_operator(bc, tau_scale) for m, bc in zip(meshes, bcs)]
         for op in self.ops[:-1]:
             if op.pc_alpha != self.alpha:

@@ -18,7 +18,12 @@ Differences (extensions, all opt-in):
     reproduce the reference (``method="cg"``, float64).
   * Solves can return their Krylov status (``return_info=True``): the
     reference discards jax's ``info`` (``sipg.py:604,910``).
-  * ``cub`` (curved-element cubature) is not supported: a ValueError.
+
+Curved meshes (``curved.project_to_curve_2d``; ``Mesh2D.is_affine`` False)
+and the cubature branch (``cub=cubature.attach_cubature(mesh)``) run the
+curved-element kernels (``curved_operator.CurvedOperator``): nodal
+quadrature without ``cub``, the cubature rule with it; the loads always use
+the nodal face rule, as in the reference.
 """
 
 from __future__ import annotations
@@ -28,6 +33,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .. import _lib
+from .curved_operator import CurvedOperator
 from .mesh import Mesh2D
 from .operator import SipgOperator, axpby, cast, dot
 
@@ -92,13 +98,16 @@ def _unflat(v, mesh, like):
     return u.cpu().numpy()
 
 
-def _check_cub(cub):
+def _op(mesh: Mesh2D, bc_types, tau_scale, cub=None):
+    """The device operator: affine kernels for straight-sided meshes without
+    ``cub``, the curved-element operator otherwise."""
     if cub is not None:
-        raise ValueError("curved-element cubature (cub=...) is not supported by the GPU SIPG path")
-
-
-def _op(mesh: Mesh2D, bc_types, tau_scale) -> SipgOperator:
+        return mesh.curved_operator(_bc_np(bc_types), tau_scale, cub)
     return mesh.device_operator(_bc_np(bc_types), tau_scale)
+
+
+def _curved(op) -> bool:
+    return isinstance(op, CurvedOperator)
 
 
 def _bc_np(bc_types):
@@ -115,8 +124,11 @@ def sipg_apply_2d(mesh: Mesh2D, u, *, bc_types, u_dir=None, tau_scale: float = 2
     given (``src/ddg/dg2d/sipg.py:304-337``).  ``M_ref`` / ``m1d_per_face``
     are accepted for signature compatibility; the device uses the reference
     element's own matrices."""
-    _check_cub(cub)
-    op = _op(mesh, bc_types, tau_scale)
+    op = _op(mesh, bc_types, tau_scale, cub)
+    if _curved(op):
+        dev = op._dev()
+        y = op.apply(_flat(u, dev)) if u_dir is None else op.apply_dir(_flat(u, dev), _flat(u_dir, dev))
+        return _unflat(y, mesh, u)
     if u_dir is None and not _is_torch(u):
         # host (Np, K) arrays: chunked copy / apply / copy-back pipeline
         return op.apply_host(u)
@@ -141,18 +153,13 @@ def sipg_neumann_load_2d(mesh: Mesh2D, q_neu, *, bc_types):
     return _unflat(op.rhs(q_neu=_flat(q_neu, op._dev())), mesh, q_neu)
 
 
-def _mass_apply(op, v):
-    """alpha J M v with alpha = 1: (alpha M + A) v - A v."""
-    y = op.apply(v, alpha=1.0)
-    axpby(-1.0, op.apply(v), 1.0, y)
-    return y
-
-
-def _dense(mesh, bc_types, tau_scale, alpha):
+def _dense(mesh, bc_types, tau_scale, alpha, cub=None):
     """Dense (alpha M + A) by applying the device operator to unit vectors
-    (``sipg_matrix_2d``, ``sipg.py:344-364``); for small meshes only."""
+    (``sipg_matrix_2d``, ``sipg.py:344-364``; with ``cub`` the mass is the
+    cubature one, ``per_element_mass`` at ``sipg.py:485-490``); for small
+    meshes only."""
     torch = _torch()
-    op = _op(mesh, bc_types, tau_scale)
+    op = _op(mesh, bc_types, tau_scale, cub)
     n = op.n
     if n > 20000:
         raise ValueError(f"dense SIPG matrix of {n} unknowns is too large; use iterative=IterativeConfig(...)")
@@ -167,14 +174,12 @@ def _dense(mesh, bc_types, tau_scale, alpha):
 
 def sipg_matrix_2d(mesh: Mesh2D, *, bc_types, tau_scale: float = 200.0, cub=None):
     """``src/ddg/dg2d/sipg.py:344-364`` (torch CUDA tensor)."""
-    _check_cub(cub)
-    return _dense(mesh, bc_types, tau_scale, 0.0)
+    return _dense(mesh, bc_types, tau_scale, 0.0, cub)
 
 
 def sipg_helmholtz_matrix_2d(mesh: Mesh2D, *, alpha, nu, bc_types, tau_scale: float = 200.0, cub=None):
     """``src/ddg/dg2d/sipg.py:460-496`` (``nu`` unused, as in the reference)."""
-    _check_cub(cub)
-    return _dense(mesh, bc_types, tau_scale, float(alpha))
+    return _dense(mesh, bc_types, tau_scale, float(alpha), cub)
 
 
 def factor_sipg_2d(mesh: Mesh2D, *, bc_types, tau_scale: float = 200.0, regularize: bool = False,
@@ -203,15 +208,27 @@ class BlockJacobiPreconditioner:
     held on the device (``sipg.py:707-715``).  Passing it to a solve on the
     same mesh / BC tags / penalty / alpha runs the fused device PCG."""
 
-    def __init__(self, op: SipgOperator, alpha: float):
+    def __init__(self, op, alpha: float):
         op.pc_build(alpha)
         self.op = op
         self.alpha = float(alpha)
         self.bc = op.bc.copy()
+        self.quad = getattr(op, "pc_quad", None)
 
     def valid_for(self, op, alpha) -> bool:
+        if _curved(op):
+            # the same blocks can be rebuilt inside another curved handle of
+            # this mesh / BC tags / penalty (e.g. the cubature solve with the
+            # nodal blocks, as the reference pairs them): any solve alpha
+            return _curved(self.op) and op.mesh is self.op.mesh and op.tau_scale == self.op.tau_scale \
+                and np.array_equal(op.bc, self.bc)
         return op is self.op and float(alpha) == self.alpha and self.op.pc_alpha == self.alpha \
             and np.array_equal(op.bc, self.bc)
+
+    def prepare(self, op):
+        """Blocks of this preconditioner in ``op`` (curved handles)."""
+        if op.pc_alpha != self.alpha or op.pc_quad != self.quad:
+            op.pc_build(self.alpha, quad=self.quad)
 
     def blocks(self):
         return self.op.pc_blocks()
@@ -226,19 +243,22 @@ class BlockJacobiPreconditioner:
 
 
 def make_sipg_block_jacobi_preconditioner(mesh: Mesh2D, *, bc_types, tau_scale: float = 200.0,
-                                          A_dense=None, matfree: bool = False):
+                                          A_dense=None, matfree: bool = False, cub=None):
     """``src/ddg/dg2d/sipg.py:718-761``.  The blocks are always computed on
     the device from the element operator (the dense and colour-probed
     variants of the reference give the same blocks), so ``A_dense`` and
-    ``matfree`` do not change the result."""
-    return BlockJacobiPreconditioner(_op(mesh, bc_types, tau_scale), 0.0)
+    ``matfree`` do not change the result.  On a curved mesh the blocks are
+    those of the nodal operator, as in the reference (it takes no ``cub``);
+    ``cub=`` (extension) gives the blocks of the cubature operator."""
+    return BlockJacobiPreconditioner(_op(mesh, bc_types, tau_scale, cub), 0.0)
 
 
 def make_helmholtz_block_jacobi_preconditioner(mesh: Mesh2D, *, alpha, nu, bc_types,
                                                tau_scale: float = 200.0, A_dense=None,
-                                               matfree: bool = False):
-    """``src/ddg/dg2d/sipg.py:764-805``."""
-    return BlockJacobiPreconditioner(_op(mesh, bc_types, tau_scale), float(alpha))
+                                               matfree: bool = False, cub=None):
+    """``src/ddg/dg2d/sipg.py:764-805`` (``cub=`` as in
+    :func:`make_sipg_block_jacobi_preconditioner`)."""
+    return BlockJacobiPreconditioner(_op(mesh, bc_types, tau_scale, cub), float(alpha))
 
 
 def _color_elements(mesh: Mesh2D):
@@ -366,6 +386,9 @@ def _iterative_solve(mesh, op, b, x0, *, alpha, shift, iterative, preconditioner
     x = torch.zeros_like(b) if x0 is None else _flat(x0, b.device)
     if iterative.method not in ("cg", "gmres"):
         raise ValueError(f"iterative method {iterative.method!r} not supported for SPD")
+    if _curved(op):
+        return x, _curved_solve(op, b, x, alpha=alpha, shift=shift, iterative=iterative,
+                                preconditioner=preconditioner)
     if iterative.precision not in ("fp64", "mixed", "mixed-restart"):
         raise ValueError(f"precision {iterative.precision!r} must be 'fp64', 'mixed' or 'mixed-restart'")
     from .multigrid import SipgMultigrid
@@ -402,6 +425,28 @@ def _iterative_solve(mesh, op, b, x0, *, alpha, shift, iterative, preconditioner
                            maxiter=iterative.maxiter, M=preconditioner)
 
 
+def _curved_solve(op, b, x, *, alpha, shift, iterative, preconditioner):
+    """Float64 solves on the curved-element operator: the device CG graph
+    (no preconditioner, or block-Jacobi from make_*_block_jacobi_* on the
+    same mesh), GMRES, or PCG around an arbitrary preconditioner callable."""
+    if iterative.precision != "fp64":
+        raise ValueError("the curved-element operator solves in float64 (precision='fp64')")
+    if iterative.method == "gmres":
+        from .krylov import gmres
+        return gmres(op, b, x, alpha=alpha, shift=shift, tol=iterative.tol, atol=iterative.atol,
+                     maxiter=iterative.maxiter, restart=iterative.restart, M=preconditioner)
+    native = preconditioner is None or (isinstance(preconditioner, BlockJacobiPreconditioner)
+                                        and preconditioner.valid_for(op, alpha))
+    if not native:
+        return _generic_pcg(op, b, x, alpha=alpha, shift=shift, tol=iterative.tol, atol=iterative.atol,
+                            maxiter=iterative.maxiter, M=preconditioner)
+    if preconditioner is not None:
+        preconditioner.prepare(op)
+    st, its, rr, bb = op.cg(b, x, tol=iterative.tol, atol=iterative.atol, maxiter=iterative.maxiter,
+                            pc=preconditioner is not None, alpha=alpha, shift=shift)
+    return SolveInfo(st, its, float(np.sqrt(max(rr, 0.0))), float(np.sqrt(bb)))
+
+
 def _dense_solve(A_factored, b):
     torch = _torch()
     _, lu, piv = A_factored
@@ -414,14 +459,13 @@ def solve_sipg_poisson_2d(mesh: Mesh2D, source, *, bc_types, u_dir=None, q_neu=N
     """``-Delta u = source`` with mixed BCs (``src/ddg/dg2d/sipg.py:812-918``),
     including the singular pure-Neumann branch (eps-shift of
     ``1e-6 ||A probe|| / ||probe||`` and a mean-free RHS, ``:891-906``)."""
-    _check_cub(cub)
     bc = _bc_np(bc_types)
-    op = _op(mesh, bc, tau_scale)
+    op = _op(mesh, bc, tau_scale, cub)
     dev = op._dev()
     b = op.rhs(_flat(source, dev), _flat(u_dir, dev), _flat(q_neu, dev))
     if iterative is None:
         if A_factored is None:
-            A_factored = factor_sipg_2d(mesh, bc_types=bc, tau_scale=tau_scale)
+            A_factored = factor_sipg_2d(mesh, bc_types=bc, tau_scale=tau_scale, cub=cub)
         u = _unflat(_dense_solve(A_factored, b), mesh, source)
         return (u, None) if return_info else u
     shift = 0.0
@@ -465,14 +509,14 @@ def solve_sipg_helmholtz_2d(mesh: Mesh2D, rhs_field, *, alpha, nu, bc_types, u_d
                             cub=None, return_info: bool = False):
     """``(alpha M - Delta) u = rhs_field`` (``src/ddg/dg2d/sipg.py:536-612``;
     ``nu`` unused, as in the reference)."""
-    _check_cub(cub)
     bc = _bc_np(bc_types)
-    op = _op(mesh, bc, tau_scale)
+    op = _op(mesh, bc, tau_scale, cub)
     dev = op._dev()
     b = op.rhs(_flat(rhs_field, dev), _flat(u_dir, dev), _flat(q_neu, dev))
     if iterative is None:
         if A_factored is None:
-            A_factored = factor_sipg_helmholtz_2d(mesh, alpha=alpha, nu=nu, bc_types=bc, tau_scale=tau_scale)
+            A_factored = factor_sipg_helmholtz_2d(mesh, alpha=alpha, nu=nu, bc_types=bc, tau_scale=tau_scale,
+                                                  cub=cub)
         u = _unflat(_dense_solve(A_factored, b), mesh, rhs_field)
         return (u, None) if return_info else u
     x, info = _iterative_solve(mesh, op, b, x0, alpha=float(alpha), shift=0.0, iterative=iterative,

@@ -306,6 +306,75 @@ int ddg_pool_retire(ddg_pool *pool, int slot, double *x, void *stream, ddg_solve
 int ddg_sipg_upload_reference(int N, const double *Dr, const double *Ds, const double *M,
                               const double *m1d, int device);
 
+/* ---- curved elements (per-node geometry, cubature) --------------------- */
+/* The operator of sipg_apply_2d on a Mesh2D whose geometric factors vary
+ * node by node (curved boundary elements, src/ddg/dg2d/curved.py:93-236),
+ * with either quadrature of sipg_bilinear_form: nodal (cub=None,
+ * src/ddg/dg2d/sipg.py:188-189, 265-280) or the cubature branch
+ * (cub=MeshCubature, src/ddg/dg2d/sipg.py:190-201, 281-299;
+ * src/ddg/dg2d/cubature.py:73-223).  Float64 only. */
+typedef struct ddg_curved_op ddg_curved_op;   /* opaque, library-owned */
+
+#define DDG_QUAD_NODAL    0
+#define DDG_QUAD_CUBATURE 1
+
+/* All pointers HOST memory, read during ddg_curved_create only.  Volume
+ * fields are the reference's (Np, K) row-major arrays, face fields
+ * (3 Nfp, K), cubature fields (Ncub, K) / (3, Nfq, K) as MeshCubature holds
+ * them. */
+typedef struct {
+    int32_t N, K, device;
+    int32_t Ncub;            /* volume cubature points; 0: nodal quadrature only   */
+    int32_t Nfq;             /* face cubature points (Ncub > 0)                   */
+    int32_t reserved;
+    double  tau_scale;       /* tau = tau_scale (N+1)^2 Fscale (first face node)  */
+    const double *Dr, *Ds, *M, *m1d;   /* reference element, as ddg_sipg_mesh_desc */
+    const int64_t *Fmask;    /* (Nfp, 3)                                          */
+    const double *rx, *sx, *ry, *sy, *J;       /* (Np, K)  mesh.py:634-644        */
+    const double *nx, *ny, *sJ, *Fscale;       /* (3 Nfp, K)  mesh.py:647-684     */
+    const int64_t *EToE, *EToF;                /* (K, 3)                          */
+    const int64_t *vmapM, *vmapP;              /* (3 Nfp K)                       */
+    const int32_t *bc_types;                   /* (K, 3)                          */
+    const double *cw;                          /* (Ncub)       MeshCubature.w     */
+    const double *Drq, *Dsq, *Lq;              /* (Ncub, Np)                      */
+    const double *cJ, *crx, *csx, *cry, *csy;  /* (Ncub, K)                       */
+    const double *face_w;                      /* (Nfq)                           */
+    const double *face_L1d;                    /* (3, Nfq, Nfp)                   */
+    const double *face_sJ;                     /* (3, Nfq, K)                     */
+} ddg_curved_desc;
+
+int ddg_curved_create(const ddg_curved_desc *desc, ddg_curved_op **out);
+int ddg_curved_destroy(ddg_curved_op *op);
+int ddg_curved_set_bc(ddg_curved_op *op, const int32_t *bc_types);
+/* y = A_quad u + alpha M_quad u (sipg_apply_2d with u_dir=None plus the
+ * Helmholtz mass of sipg.py:593-601, cubature_mass_apply for quad 1);
+ * element-major float64 device vectors. */
+int ddg_curved_apply(ddg_curved_op *op, int quad, double alpha, const double *u, double *y, void *stream);
+/* y = d a_quad(u, v; u_dir) / d v at v = 0: sipg_apply_2d with a
+ * non-homogeneous Dirichlet ghost u_dir (sipg.py:216-233, 304-337), i.e.
+ * A_quad u plus the Dirichlet load of u_dir by the same face rule.  u may be
+ * null (zero): y is then the load alone (sipg.py:398-417 for quad 0). */
+int ddg_curved_apply_dir(ddg_curved_op *op, int quad, const double *u, const double *u_dir, double *y,
+                         void *stream);
+/* y = M_quad f (mesh.J * (M_ref @ f) or cubature_mass_apply). */
+int ddg_curved_mass(ddg_curved_op *op, int quad, const double *f, double *y, void *stream);
+/* rhs = M_quad f - L_D(u_dir) + L_N(q_neu) (sipg.py:564-574, 851-864); the
+ * loads use the nodal face rule, as sipg_dirichlet_load_2d /
+ * sipg_neumann_load_2d do (sipg.py:398-453).  f, u_dir, q_neu may be null. */
+int ddg_curved_rhs(ddg_curved_op *op, int quad, const double *f, const double *u_dir,
+                   const double *q_neu, double *rhs, void *stream);
+/* Block-Jacobi of (alpha M + A)_quad: diagonal blocks by coloured probing
+ * of the apply (sipg.py:651-704), explicit inverses (sipg.py:707-715). */
+int ddg_curved_pc_build(ddg_curved_op *op, int quad, double alpha, void *stream);
+int ddg_curved_pc_apply(ddg_curved_op *op, const double *r, double *z, void *stream);
+/* (K, Np, Np) row-major diagonal blocks of the last pc_build. */
+int ddg_curved_pc_blocks(ddg_curved_op *op, double *blocks, void *stream);
+/* float64 CG on (alpha M + A + shift I)_quad x = b, the stopping rule of
+ * ddg_sipg_cg; cfg->pc = DDG_PC_JACOBI uses the last pc_build.  The loop
+ * runs as a CUDA graph with a conditional while node. */
+int ddg_curved_cg(ddg_curved_op *op, int quad, const ddg_cg_config *cfg, const double *b,
+                  double *x, void *stream, ddg_solve_info *info);
+
 /* ---- small vector helpers (device) ------------------------------------ */
 /* y = a*x + b*y  (float64) */
 int ddg_axpby(int64_t n, double a, const double *x, double b, double *y, void *stream);
