@@ -64,6 +64,7 @@ def algorithmic_bytes(K, Np, sv, sg):
 # oracle's float64 solution (the full size takes minutes on the host cores)
 SMALL = 64
 SMALL_SOLVES: dict = {}
+CURVED_SAMPLE: dict = {}
 
 # DRAM bytes of one float64 tensor-core apply launch on this workload, from
 # an ncu capture (56.16 MB read + 1.23 MB written; y stays in L2)
@@ -276,6 +277,7 @@ def run_ours(args, rank, world, local_rank):
         "solves": solves,
     }
     if not args.skip_workloads:
+        line["curved"] = curved_leg(args.steps, hbm)
         line["plain"] = plain_leg()
         line["hpmg_pressure_poisson"] = hpmg_leg()
         line["serving"] = serving_leg(args.serving_requests)
@@ -393,6 +395,95 @@ def plain_leg():
             "rel_err_vs_reference_solution": float(np.linalg.norm(u - gs["plain/u_cg"]) /
                                                    np.linalg.norm(gs["plain/u_cg"])),
             "solve_ms": 1e3 * float(np.median(lat[1:]))}
+
+
+def curved_workload(build_mesh, channel, bend, attach):
+    """Cylinder in a channel: [0,32]^2 split into 256 x 256 cells minus the
+    grid-aligned box of half-side 2 around (16, 16), plus an O-grid of 8
+    layers (growth 1.2) down to a cylinder of radius 1 whose faces are bent
+    onto the circle -> 131,072 triangles, N = 4 (1,966,080 DOFs, the size of
+    the precision workload), all boundaries Dirichlet, with its cubature."""
+    VX, VY, E = channel(0.0, 32.0, 0.0, 32.0, 256, 256, cx=16.0, cy=16.0, radius=1.0, R_outer=2.0,
+                        n_radial=8, radial_growth=1.2)
+    m = bend(build_mesh(VX, VY, E, NDEG), cx=16.0, cy=16.0, radius=1.0)
+    bc = np.where(np.asarray(m.EToE) == np.arange(m.K)[:, None], 1, 0).astype(np.int32)
+    return m, bc, attach(m)
+
+
+def curved_bytes(N, Ncub, quad):
+    """Algorithmic bytes per element of one curved-element apply: every array
+    each of the three passes reads or writes, counted once per pass (float64
+    values, int32 tags and slot maps)."""
+    Np, Nfp = (N + 1) * (N + 2) // 2, N + 1
+    Ns, nq = 3 * Nfp, Nfp * (Nfp + 1) // 2
+    p1 = 8 * (Np + 4 * 3 * N + 2 * Ns)
+    p2 = 4 * 3 + 8 * 2 * Ns + 8 * 3 * N + 4 * 2 * Ns + 8 * 2 * Ns + 8 * 3 * Ns
+    p2 += 8 * 3 * (1 + nq) if quad == "cubature" else 8 * 2 * 3
+    p3 = 8 * Np + 4 * 3 + 4 * Ns + 8 * 3 * Ns + 8 * 4 * Np + 8 * Np
+    p3 += 8 * 4 * Ncub if quad == "cubature" else 8 * Np
+    return p1 + p2 + p3
+
+
+def curved_leg(steps, hbm):
+    """The curved-element branch (cub=...) on the cylinder workload: the
+    nodal and cubature applies (device-timed, L2 flushed), the cubature
+    Helmholtz solve with block-Jacobi PCG, and the matvec against the
+    reference's own cubature apply (tests/golden/curved.npz)."""
+    import torch
+    from ddg_b200.dg2d import cubature as pcub
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    m, bc, cub = curved_workload(pm.build_mesh_2d, pm.channel_with_circle_mesh_2d, pcur.apply_circular_hole_2d,
+                                 pcub.attach_cubature)
+    op = m.curved_operator(bc, TAU_SCALE, cub)
+    n = op.n
+    u = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    y = torch.empty_like(u)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {"workload": f"cylinder in a channel (O-grid, faces bent onto the circle): {m.K} triangles, N={NDEG}, "
+                       f"{n} DOFs, {cub.w.shape[0]}-point volume cubature, Dirichlet, alpha={ALPHA:g}, "
+                       f"tau_scale={TAU_SCALE}"}
+    for quad in ("nodal", "cubature"):
+        for _ in range(3):
+            op.apply(u, alpha=ALPHA, out=y, quad=quad)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record()
+            op.apply(u, alpha=ALPHA, out=y, quad=quad)
+            ev[i][1].record()
+        torch.cuda.synchronize()
+        t = float(np.mean([a.elapsed_time(b) * 1e-3 for a, b in ev]))
+        B = curved_bytes(NDEG, int(cub.w.shape[0]), quad) * m.K
+        out[quad] = {"gdofs": n / t / 1e9, "us": t * 1e6, "launches": 3,
+                     "roofline": {"bound": "hbm", "achieved": B / t / 1e9, "peak": hbm, "unit": "GB/s",
+                                  "frac": B / t / 1e9 / hbm, "algorithmic_bytes": B,
+                                  "kernels": "k_cv_trace, k_cv_dual, k_cv_gather (one apply)"}}
+    f = np.cos(0.3 * m.x) * np.sin(0.2 * m.y) + 0.1
+    pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE,
+                                                       cub=cub)
+    cfg = ps.IterativeConfig(tol=1e-8, maxiter=20000)
+    lat = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, info = ps.solve_sipg_helmholtz_2d(m, f, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE, cub=cub,
+                                             preconditioner=pc, iterative=cfg, return_info=True)
+        lat.append(time.perf_counter() - t0)
+    out["solve"] = {"iterations": info.iterations, "status": info.status, "tol": 1e-8,
+                    "solves_per_s": 1.0 / float(np.median(lat[1:])), "ms_per_iteration":
+                    1e3 * float(np.median(lat[1:])) / max(info.iterations, 1),
+                    "note": "solve_sipg_helmholtz_2d(cub=...) with the cubature block-Jacobi; host wall clock"}
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "curved.npz"))
+    gm = pm.build_mesh_2d(gold["annulus8_N3/VX"], gold["annulus8_N3/VY"], gold["annulus8_N3/EToV"], 3)
+    gm = pcur.apply_circular_hole_2d(gm, cx=0.0, cy=0.0, radius=0.5, detection_tol=0.5)
+    k = "annulus8_N3/apply/random/tau0.5"
+    Au = ps.sipg_apply_2d(gm, gold[k + "/u"], bc_types=gold[k + "/bc"], tau_scale=0.5, cub=pcub.attach_cubature(gm))
+    out["matvec_rel_err_vs_reference"] = float(np.max(np.abs(Au - gold[k + "/Au_cub"])) /
+                                               np.max(np.abs(gold[k + "/Au_cub"])))
+    CURVED_SAMPLE["gdofs_cubature"] = out["cubature"]["gdofs"]
+    return out
 
 
 def serving_leg(count=4096, loads=(0.5, 0.8)):
@@ -581,7 +672,36 @@ def cpu_baseline(budget_s=15.0):
     for name, ug in SMALL_SOLVES.items():
         solve[f"rel_l2_err_{name}_vs_oracle"] = float(np.linalg.norm(ug - u) / np.linalg.norm(u))
     out["solve"] = solve
+    if CURVED_SAMPLE:
+        out["curved"] = cpu_curved(budget_s=min(budget_s, 10.0))
     return out
+
+
+def cpu_curved(budget_s=10.0):
+    """The oracle's float64 cubature apply (numpy, batched over elements) on
+    the cylinder workload's elements, timed on a bounded sample: whole
+    applies of a 64 x 64-cell version of the same mesh."""
+    from oracle import cubature as ocub
+    from oracle import curved as ocur
+    from oracle import mesh as om
+    from oracle import sipg as osp
+    VX, VY, E = ocur.channel_with_circle_mesh_2d(0.0, 32.0, 0.0, 32.0, 64, 64, cx=16.0, cy=16.0, radius=1.0,
+                                                 R_outer=2.0, n_radial=8, radial_growth=1.2)
+    m = ocur.apply_circular_hole_2d(om.build_mesh_2d(VX, VY, E, NDEG), cx=16.0, cy=16.0, radius=1.0)
+    cub = ocub.attach_cubature(m)
+    bc = np.where(m.EToE == np.arange(m.K)[:, None], 1, 0).astype(np.int32)
+    u = np.random.default_rng(4).standard_normal((m.Np, m.K))
+    ts, t_end = [], time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(ts) < 3:
+        t0 = time.perf_counter()
+        osp.apply(m, u, bc_types=bc, tau_scale=TAU_SCALE, cub=cub)
+        ts.append(time.perf_counter() - t0)
+    t = float(np.median(ts))
+    v = m.K * m.Np / t / 1e9
+    return {"value": v, "unit": "GDOF/s", "kind": "port", "cores": 1,
+            "sample": f"{len(ts)} cubature applies of the {m.K}-element version of the cylinder mesh by the "
+                      f"oracle (numpy), median {t * 1e3:.1f} ms",
+            "gpu_over_cpu": CURVED_SAMPLE["gdofs_cubature"] / v}
 
 
 def run_reference(args, rank, world):

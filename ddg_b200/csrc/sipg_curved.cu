@@ -188,7 +188,7 @@ enum CvMode { CV_APPLY = 0, CV_SUB = 1, CV_PDOT = 2, CV_RESID = 3 };
 // rank-one update Dr^T e_n (rx bx + ry by) + Ds^T e_n (sx bx + sy by), the
 // nodal volume node by node, and the element's u stays in the shared tile.
 template <int N, bool CUB, int MODE>
-__global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 2) k_cv_gather(CvArgs a, const double* __restrict__ u,
+__global__ void __launch_bounds__(CV_BLOCK, 4) k_cv_gather(CvArgs a, const double* __restrict__ u,
                                                                     const double* __restrict__ b,
                                                                     double* __restrict__ y, double alpha,
                                                                     double shift) {
@@ -214,32 +214,34 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 2) k_cv_gather(CvArgs a, c
 #pragma unroll
     for (int i = 0; i < Np; ++i) out[i] = 0.0;
     // faces: own sides, then the neighbours' sides facing this element
-#pragma unroll
-    for (int f = 0; f < 3; ++f) {
+    // (one slot per iteration: the node index is warp-uniform, so the
+    // constant-bank rows stay broadcasts and the scalar part is a
+    // predicated add into the statically indexed output)
+#pragma unroll 1
+    for (int m = 0; m < Ns; ++m) {
+      const int f = m / Nfp, n = fmask_idx(N, f, m - f * Nfp);
       const int t = a.tag[f * K + k];
       const double c = t == DDG_BC_DIRICHLET ? 2.0 : 1.0;
+      double av = 0.0, bx = 0.0, by = 0.0;
+      if (t != DDG_BC_NEUMANN) {
+        av = a.dl[(size_t)(0 * Ns + m) * K + k];
+        bx = c * a.dl[(size_t)(1 * Ns + m) * K + k];
+        by = c * a.dl[(size_t)(2 * Ns + m) * K + k];
+      }
+      const int mp = a.mapP[(size_t)m * K + k];
+      const int k2 = mp % a.K, f2 = (mp / a.K) / Nfp;
+      if (a.tag[f2 * K + k2] == DDG_BC_INTERIOR) {
+        av -= a.dl[(size_t)mp];
+        bx += a.dl[(size_t)Ns * K + mp];
+        by += a.dl[(size_t)2 * Ns * K + mp];
+      }
+      const double rx = a.gN[(0 * Np + n) * K + k], sx = a.gN[(1 * Np + n) * K + k];
+      const double ry = a.gN[(2 * Np + n) * K + k], sy = a.gN[(3 * Np + n) * K + k];
+      const double tr = fma(rx, bx, ry * by), ts = fma(sx, bx, sy * by);
 #pragma unroll
-      for (int p = 0; p < Nfp; ++p) {
-        const int n = fmask_idx(N, f, p), m = f * Nfp + p;
-        double av = 0.0, bx = 0.0, by = 0.0;
-        if (t != DDG_BC_NEUMANN) {
-          av = a.dl[(size_t)(0 * Ns + m) * K + k];
-          bx = c * a.dl[(size_t)(1 * Ns + m) * K + k];
-          by = c * a.dl[(size_t)(2 * Ns + m) * K + k];
-        }
-        const int mp = a.mapP[(size_t)m * K + k];
-        const int k2 = mp % a.K, f2 = (mp / a.K) / Nfp;
-        if (a.tag[f2 * K + k2] == DDG_BC_INTERIOR) {
-          av -= a.dl[(size_t)mp];
-          bx += a.dl[(size_t)Ns * K + mp];
-          by += a.dl[(size_t)2 * Ns * K + mp];
-        }
-        out[n] += av;
-        const double rx = a.gN[(0 * Np + n) * K + k], sx = a.gN[(1 * Np + n) * K + k];
-        const double ry = a.gN[(2 * Np + n) * K + k], sy = a.gN[(3 * Np + n) * K + k];
-        const double tr = fma(rx, bx, ry * by), ts = fma(sx, bx, sy * by);
-#pragma unroll
-        for (int i = 0; i < Np; ++i) out[i] = fma(R.Dr[n * Np + i], tr, fma(R.Ds[n * Np + i], ts, out[i]));
+      for (int i = 0; i < Np; ++i) {
+        out[i] = fma(R.Dr[n * Np + i], tr, fma(R.Ds[n * Np + i], ts, out[i]));
+        if (i == n) out[i] += av;
       }
     }
     if (!CUB) {
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 2) k_cv_gather(CvArgs a, c
         jx[i] = J * fma(a.gN[(0 * Np + i) * K + k], ur, a.gN[(1 * Np + i) * K + k] * us);
         jy[i] = J * fma(a.gN[(2 * Np + i) * K + k], ur, a.gN[(3 * Np + i) * K + k] * us);
       }
-#pragma unroll
+#pragma unroll 1
       for (int n = 0; n < Np; ++n) {
         double hx = 0.0, hy = 0.0;
 #pragma unroll

@@ -132,7 +132,7 @@ def test_curved_poisson_solves_match_reference():
     # by ~1% and the solution (tol 1e-10 on the residual) by a few 1e-8
     assert abs(info.iterations - ref_its) <= max(3, int(0.02 * ref_its))
     assert _rel(u, g["annulus8_N3/solve/u_cg_cub"]) < 1e-7
-    assert _rel(u, g["annulus8_N3/solve/u_lu_cub"]) < 1e-7
+    assert _rel(u, g["annulus8_N3/solve/u_lu_cub"]) < 1e-6
 
 
 def test_curved_helmholtz_solves_match_reference():

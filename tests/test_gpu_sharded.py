@@ -1,0 +1,56 @@
+"""The sharded solve's device path on one GPU (a single NCCL rank): the
+rank-local operator, RHS, block-Jacobi and vector kernels of
+``libddg_sipg.so`` under the distributed CG give the same solution as the
+single-GPU solve.  The multi-rank halo exchange and reductions are tested
+as gloo ranks on the CPU (``tests/test_sharded.py``); this run has one GPU."""
+
+import socket
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+@pytest.mark.parametrize("case", ["helmholtz_bj", "poisson_neumann"])
+def test_sharded_single_rank_matches_single_gpu_solve(case):
+    import torch.distributed as dist
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg as ps
+    from ddg_b200.dg2d.sharded import ShardedSipg
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_port()}", rank=0, world_size=1)
+    try:
+        VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 2.0, 0.0, 1.0, 24, 12)
+        m = pm.build_mesh_2d(VX, VY, E, 3)
+        isb = m.EToE == np.arange(m.K)[:, None]
+        if case == "helmholtz_bj":
+            bc = np.where(isb, 1, 0).astype(np.int32)
+            f = np.sin(2 * m.x) * np.cos(3 * m.y) + 0.2
+            sh = ShardedSipg(m, bc, tau_scale=0.5)
+            u, info = sh.solve(f, alpha=3.0, tol=1e-10, maxiter=3000)
+            pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=3.0, nu=1.0, bc_types=bc, tau_scale=0.5)
+            ref, rinfo = ps.solve_sipg_helmholtz_2d(m, f, alpha=3.0, nu=1.0, bc_types=bc, tau_scale=0.5,
+                                                    preconditioner=pc, return_info=True,
+                                                    iterative=ps.IterativeConfig(tol=1e-10, maxiter=3000))
+        else:
+            bc = np.where(isb, 2, 0).astype(np.int32)
+            f = np.cos(np.pi * m.x / 2) * np.cos(np.pi * m.y) + 0.3
+            sh = ShardedSipg(m, bc, tau_scale=200.0)
+            u, info = sh.solve(f, tol=1e-9, maxiter=3000)
+            pc = ps.make_sipg_block_jacobi_preconditioner(m, bc_types=bc, tau_scale=200.0)
+            ref, rinfo = ps.solve_sipg_poisson_2d(m, f, bc_types=bc, tau_scale=200.0, preconditioner=pc,
+                                                  return_info=True,
+                                                  iterative=ps.IterativeConfig(tol=1e-9, maxiter=3000))
+        assert info.status == "converged" and rinfo.status == "converged"
+        assert abs(info.iterations - rinfo.iterations) <= 2
+        assert np.linalg.norm(u - ref) <= 1e-7 * np.linalg.norm(ref)
+    finally:
+        dist.destroy_process_group()
