@@ -578,7 +578,8 @@ def profile_kernels(args):
     sets; conditional graphs hide their kernels from profilers), including
     the block-Jacobi set-up; `mg`: V-cycle applies of the pressure-Poisson
     workload's hp-multigrid; `serving`: a 64-request stream through the
-    pools; `adjoint`: one gradient of the differentiation workload."""
+    pools; `adjoint`: one gradient of the differentiation workload;
+    `curved`: nodal then cubature applies of the curved-element workload."""
     import torch
     from ddg_b200.dg2d import mesh as pm
     from ddg_b200.dg2d import sipg as ps
@@ -616,6 +617,18 @@ def profile_kernels(args):
         done = eng.run(serving.make_requests(count=64, seed=0), realtime=False)
         eng.close()
         print("serving", len(done), flush=True)
+    elif what == "curved":
+        from ddg_b200.dg2d import cubature as pcub
+        from ddg_b200.dg2d import curved as pcur
+        m, bc, cub = curved_workload(pm.build_mesh_2d, pm.channel_with_circle_mesh_2d, pcur.apply_circular_hole_2d,
+                                     pcub.attach_cubature)
+        op = m.curved_operator(bc, TAU_SCALE, cub)
+        u = torch.randn(op.n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+        for quad in ("nodal", "cubature"):
+            for _ in range(args.profile_reps):
+                op.apply(u, alpha=ALPHA, quad=quad)
+        torch.cuda.synchronize()
+        print("curved applies done", flush=True)
     elif what == "adjoint":
         from ddg_b200 import adjoint
         VX, VY, E = pm.uniform_rectangle_mesh_2d(0.0, 1.0, 0.0, 1.0, 64, 64)
@@ -752,7 +765,8 @@ def main():
     ap.add_argument("--profile-apply", choices=["fp64", "fp32"], default=None,
                     help="only stand-alone applies of one precision (for a profiler's capture of that kernel)")
     ap.add_argument("--profile-reps", type=int, default=5)
-    ap.add_argument("--profile-kernels", choices=["cg-fp64", "cg-fp32", "mg", "serving", "adjoint"], default=None,
+    ap.add_argument("--profile-kernels", choices=["cg-fp64", "cg-fp32", "mg", "serving", "adjoint", "curved"],
+                    default=None,
                     help="only a short run of those kernels (for a profiler's per-kernel capture)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

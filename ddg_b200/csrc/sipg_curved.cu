@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(CV_BLOCK) k_cv_trace(CvArgs a, const double* _
 
 // ---------------------------------------------------------------- pass 2
 template <int N, bool CUB>
-__global__ void __launch_bounds__(CV_BLOCK) k_cv_dual(CvArgs a, const double* __restrict__ u,
+__global__ void __launch_bounds__(CV_BLOCK, CUB ? 4 : 8) k_cv_dual(CvArgs a, const double* __restrict__ u,
                                                       const double* __restrict__ udir) {
   constexpr int Np = CvDim<N>::Np, Nfp = CvDim<N>::Nfp, Ns = CvDim<N>::Ns, NQ = CvDim<N>::NQ;
   if (a.ctl && a.gate && a.ctl->cont == 0) return;
@@ -181,14 +181,14 @@ __global__ void __launch_bounds__(CV_BLOCK) k_cv_dual(CvArgs a, const double* __
 // ---------------------------------------------------------------- pass 3
 enum CvMode { CV_APPLY = 0, CV_SUB = 1, CV_PDOT = 2, CV_RESID = 3 };
 
-// dynamic shared memory: the element tile (CV_BLOCK Np doubles), then the
-// cubature matrices Drq, Dsq, Lq (3 Ncub Np doubles; CUB only).
+// dynamic shared memory: the element tile (CV_BLOCK Np doubles), then (CUB)
+// the tile of the cubature volume term computed by k_cv_cubvol.
 // Register budget: only the output row and, for the nodal volume, J grad u
 // are held per thread.  The gradient part of every face slot is applied as a
 // rank-one update Dr^T e_n (rx bx + ry by) + Ds^T e_n (sx bx + sy by), the
 // nodal volume node by node, and the element's u stays in the shared tile.
 template <int N, bool CUB, int MODE>
-__global__ void __launch_bounds__(CV_BLOCK, 4) k_cv_gather(CvArgs a, const double* __restrict__ u,
+__global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 4) k_cv_gather(CvArgs a, const double* __restrict__ u,
                                                                     const double* __restrict__ b,
                                                                     double* __restrict__ y, double alpha,
                                                                     double shift) {
@@ -200,8 +200,7 @@ __global__ void __launch_bounds__(CV_BLOCK, 4) k_cv_gather(CvArgs a, const doubl
   double* s_m = s_dyn + CV_BLOCK * Np;
   const int k0 = blockIdx.x * CV_BLOCK, nk = min(CV_BLOCK, a.K - k0);
   stage_tile<Np>(u, k0, nk, s_u);
-  if (CUB)
-    for (int i = threadIdx.x; i < 3 * a.Ncub * Np; i += CV_BLOCK) s_m[i] = a.cMat[i];
+  if (CUB) stage_tile<Np>(a.vol, k0, nk, s_m);
   __syncthreads();
   const bool active = (int)threadIdx.x < nk;
   const int k = k0 + threadIdx.x;
@@ -283,31 +282,10 @@ __global__ void __launch_bounds__(CV_BLOCK, 4) k_cv_gather(CvArgs a, const doubl
         }
       }
     } else {
-      // cubature volume (and mass): sum over the points of the staged
-      // reference derivatives / basis values
-      const double* Drq = s_m;
-      const double* Dsq = s_m + a.Ncub * Np;
-      const double* Lq = s_m + 2 * a.Ncub * Np;
-      double uv[Np];
+      // cubature volume and mass: computed by k_cv_cubvol into a.vol
+      const double* ve = s_m + threadIdx.x * Np;
 #pragma unroll
-      for (int j = 0; j < Np; ++j) uv[j] = ue[j];
-      for (int q = 0; q < a.Ncub; ++q) {
-        double ur = 0.0, us = 0.0, uq = 0.0;
-#pragma unroll
-        for (int j = 0; j < Np; ++j) {
-          ur = fma(Drq[q * Np + j], uv[j], ur);
-          us = fma(Dsq[q * Np + j], uv[j], us);
-          uq = fma(Lq[q * Np + j], uv[j], uq);
-        }
-        const double Grr = a.cG[(size_t)(0 * a.Ncub + q) * K + k];
-        const double Grs = a.cG[(size_t)(1 * a.Ncub + q) * K + k];
-        const double Gss = a.cG[(size_t)(2 * a.Ncub + q) * K + k];
-        const double wJ = a.cG[(size_t)(3 * a.Ncub + q) * K + k];
-        const double vr = fma(Grr, ur, Grs * us), vs = fma(Grs, ur, Gss * us), vm = alpha * wJ * uq;
-#pragma unroll
-        for (int i = 0; i < Np; ++i)
-          out[i] = fma(Drq[q * Np + i], vr, fma(Dsq[q * Np + i], vs, fma(Lq[q * Np + i], vm, out[i])));
-      }
+      for (int i = 0; i < Np; ++i) out[i] += ve[i];
     }
     if (shift != 0.0) {
 #pragma unroll
@@ -365,6 +343,75 @@ __global__ void __launch_bounds__(CV_BLOCK, 4) k_cv_gather(CvArgs a, const doubl
     }
     c->ticket = 0u;
   }
+}
+
+// ------------------------------------------------------- cubature volume
+// vol = sum_q Drq^T (G_rr ur + G_rs us) + Dsq^T (G_rs ur + G_ss us)
+//       + alpha Lq^T (wJ Lq u)            (sipg.py:190-201; cubature.py:243-254)
+// CV_TPE threads per element split the cubature points (point q to thread
+// q mod CV_TPE) and add their partial rows with warp shuffles, so the G
+// table streams through many more warps than one thread per element allows.
+constexpr int CV_TPE = 4;
+template <int N>
+__global__ void __launch_bounds__(CV_BLOCK, 2) k_cv_cubvol(CvArgs a, const double* __restrict__ u, double alpha) {
+  constexpr int Np = CvDim<N>::Np, EPB = CV_BLOCK / CV_TPE;
+  if (a.ctl && a.gate && a.ctl->cont == 0) return;
+  extern __shared__ __align__(16) double s_dyn[];
+  double* s_u = s_dyn;                 // EPB Np
+  double* s_m = s_dyn + EPB * Np;      // Drq, Dsq, Lq
+  const int k0 = blockIdx.x * EPB, nk = min(EPB, a.K - k0);
+  stage_tile<Np>(u, k0, nk, s_u);
+  for (int i = threadIdx.x; i < 3 * a.Ncub * Np; i += CV_BLOCK) s_m[i] = a.cMat[i];
+  __syncthreads();
+  const int e = threadIdx.x / CV_TPE, t = threadIdx.x % CV_TPE;
+  const bool active = e < nk;
+  const int k = k0 + (active ? e : 0);
+  const size_t K = (size_t)a.K;
+  const double* Drq = s_m;
+  const double* Dsq = s_m + a.Ncub * Np;
+  const double* Lq = s_m + 2 * a.Ncub * Np;
+  double uv[Np], out[Np];
+#pragma unroll
+  for (int j = 0; j < Np; ++j) {
+    uv[j] = active ? s_u[e * Np + j] : 0.0;
+    out[j] = 0.0;
+  }
+#pragma unroll 1
+  for (int q = t; q < a.Ncub; q += CV_TPE) {
+    double ur = 0.0, us = 0.0, uq = 0.0;
+#pragma unroll
+    for (int j = 0; j < Np; ++j) {
+      ur = fma(Drq[q * Np + j], uv[j], ur);
+      us = fma(Dsq[q * Np + j], uv[j], us);
+      uq = fma(Lq[q * Np + j], uv[j], uq);
+    }
+    double Grr = 0.0, Grs = 0.0, Gss = 0.0, wJ = 0.0;
+    if (active) {
+      Grr = a.cG[(size_t)(0 * a.Ncub + q) * K + k];
+      Grs = a.cG[(size_t)(1 * a.Ncub + q) * K + k];
+      Gss = a.cG[(size_t)(2 * a.Ncub + q) * K + k];
+      wJ = a.cG[(size_t)(3 * a.Ncub + q) * K + k];
+    }
+    const double vr = fma(Grr, ur, Grs * us), vs = fma(Grs, ur, Gss * us), vm = alpha * wJ * uq;
+#pragma unroll
+    for (int i = 0; i < Np; ++i)
+      out[i] = fma(Drq[q * Np + i], vr, fma(Dsq[q * Np + i], vs, fma(Lq[q * Np + i], vm, out[i])));
+  }
+  // the CV_TPE threads of an element are adjacent lanes of one warp
+#pragma unroll
+  for (int i = 0; i < Np; ++i) {
+#pragma unroll
+    for (int o = 1; o < CV_TPE; o <<= 1) out[i] += __shfl_xor_sync(0xffffffffu, out[i], o);
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < Np; ++i)
+      if (i % CV_TPE == t) s_u[e * Np + i] = out[i];
+  }
+  __syncthreads();
+  const size_t off = (size_t)k0 * Np;
+  for (int i = threadIdx.x; i < nk * Np; i += CV_BLOCK) a.vol[off + i] = s_u[i];
 }
 
 // ------------------------------------------------------------- mass, loads
@@ -567,7 +614,14 @@ template <int N, bool CUB, int MODE>
 cudaError_t gather_n(const CvArgs& a, const double* u, const double* b, double* y, double alpha, double shift,
                      cudaStream_t s) {
   constexpr int Np = CvDim<N>::Np;
-  const size_t smem = (size_t)(CV_BLOCK * Np + (CUB ? 3 * a.Ncub * Np : 0)) * sizeof(double);
+  const size_t smem = (size_t)(CV_BLOCK * Np * (CUB ? 2 : 1)) * sizeof(double);
+  if (CUB) {
+    constexpr int EPB = CV_BLOCK / CV_TPE;
+    const size_t sv = (size_t)(EPB * Np + 3 * a.Ncub * Np) * sizeof(double);
+    k_cv_cubvol<N><<<(a.K + EPB - 1) / EPB, CV_BLOCK, sv, s>>>(a, u, alpha);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   k_cv_gather<N, CUB, MODE><<<(a.K + CV_BLOCK - 1) / CV_BLOCK, CV_BLOCK, smem, s>>>(a, u, b, y, alpha, shift);
   return cudaGetLastError();
 }
@@ -631,6 +685,7 @@ cudaError_t cv_prepare_n() {
   CV_A((k_cv_gather<N, false, CV_SUB>));
   CV_A((k_cv_gather<N, false, CV_PDOT>));
   CV_A((k_cv_gather<N, false, CV_RESID>));
+  CV_A((k_cv_cubvol<N>));
   CV_A((k_cv_mass<N, true>));
   CV_A((k_cv_mass<N, false>));
 #undef CV_A

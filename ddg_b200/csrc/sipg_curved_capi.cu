@@ -57,7 +57,7 @@ struct ddg_curved_op {
   double tau_scale = 0.0;
   double *gN = nullptr, *fN = nullptr, *sJ0 = nullptr, *tauF = nullptr;
   double *cG = nullptr, *cQ = nullptr, *cMat = nullptr;
-  double *tr = nullptr, *dl = nullptr, *zero = nullptr;
+  double *tr = nullptr, *dl = nullptr, *zero = nullptr, *vol = nullptr;
   int *tag = nullptr, *slotP = nullptr, *mapP = nullptr, *colour = nullptr;
   unsigned int* status = nullptr;
   CgCtl* ctl = nullptr;
@@ -91,6 +91,7 @@ CvArgs cv_args(const ddg_curved_op* op, int gate) {
   a.cMat = op->cMat;
   a.tr = op->tr;
   a.dl = op->dl;
+  a.vol = op->vol;
   a.ctl = op->ctl;
   a.partA = op->partA;
   a.partB = op->partB;
@@ -134,7 +135,7 @@ void cv_free(ddg_curved_op* op) {
   }
   op->graphs.clear();
   for (void* ptr : {(void*)op->gN, (void*)op->fN, (void*)op->sJ0, (void*)op->tauF, (void*)op->cG, (void*)op->cQ,
-                    (void*)op->cMat, (void*)op->tr, (void*)op->dl, (void*)op->zero, (void*)op->tag,
+                    (void*)op->cMat, (void*)op->tr, (void*)op->dl, (void*)op->zero, (void*)op->vol, (void*)op->tag,
                     (void*)op->slotP, (void*)op->mapP, (void*)op->colour, (void*)op->status, (void*)op->ctl,
                     (void*)op->partA, (void*)op->partB, (void*)op->blocks, (void*)op->binv, (void*)op->x,
                     (void*)op->r, (void*)op->z, (void*)op->p, (void*)op->Ap, (void*)op->b})
@@ -232,7 +233,7 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
   if (Ncub > 0 && (Nfq < 1 || !d->cw || !d->Drq || !d->Dsq || !d->Lq || !d->cJ || !d->crx || !d->csx || !d->cry ||
                    !d->csy || !d->face_w || !d->face_L1d || !d->face_sJ))
     return fail(DDG_ERR_INVALID, "ddg_curved_create: cubature arrays missing");
-  if ((size_t)(128 * Np + 3 * (size_t)Ncub * Np) * sizeof(double) > (size_t)CV_SMEM_LIMIT)
+  if ((size_t)(32 * Np + 3 * (size_t)Ncub * Np) * sizeof(double) > (size_t)CV_SMEM_LIMIT)
     return fail(DDG_ERR_UNSUPPORTED, "cubature rule too large for the staged kernels (Ncub = " + std::to_string(Ncub) +
                                          ")");
   for (int p = 0; p < Nfp; ++p)
@@ -369,6 +370,7 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
     ALLOC(op->cG, cG.size() * 8);
     ALLOC(op->cQ, cQ.size() * 8);
     ALLOC(op->cMat, cMat.size() * 8);
+    ALLOC(op->vol, KN * 8);
   }
   UPLOAD(op->gN, gN);
   UPLOAD(op->fN, fN);

@@ -145,6 +145,7 @@ struct CvArgs {
   const double* cMat;  // [3][Ncub][Np] Drq, Dsq, Lq
   double* tr;          // [2][3Nfp][K] gradient traces (pass 1)
   double* dl;          // [3][3Nfp][K] face duals (pass 2)
+  double* vol;         // element-major cubature volume (+ mass) term of the gather pass
   CgCtl* ctl;          // CG control block (PDOT, RESID; gating inside CG graphs)
   double* partA;       // per-block partials
   double* partB;

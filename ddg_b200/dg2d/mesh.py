@@ -247,8 +247,12 @@ class Mesh2D:
         bc = np.ascontiguousarray(np.asarray(bc_types), dtype=np.int32)
         if bc.shape != (self.K, 3):
             raise ValueError(f"bc_types must have shape (K, 3) = ({self.K}, 3), got {bc.shape}")
-        if cub is not None and cub.mesh is not self:
-            raise ValueError("cub was attached to a different mesh")
+        if cub is not None:
+            from .cubature import MeshCubature
+            if not isinstance(cub, MeshCubature):
+                raise ValueError("cub must be the MeshCubature of attach_cubature(mesh)")
+            if cub.mesh is not self:
+                raise ValueError("cub was attached to a different mesh")
         key = ("curved", float(tau_scale), dev, bc.tobytes(), id(cub) if cub is not None else None)
         op = self._ops.pop(key, None)
         if op is None or op.cub is not cub:
