@@ -67,6 +67,18 @@ CV_REF(5)
 namespace cv {
 
 constexpr int CV_BLOCK = 128;
+constexpr int CV_GQ = 4;    // cubature points per staged chunk of the G table
+
+__host__ __device__ constexpr int cv_even(int n) { return (n + 1) & ~1; }
+
+// asynchronous 16-byte global -> shared copies (no registers held in flight)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// every group but the most recent one has completed
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int N>
 struct CvDim {
@@ -182,13 +194,15 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 4 : 8) k_cv_dual(CvArgs a, con
 enum CvMode { CV_APPLY = 0, CV_SUB = 1, CV_PDOT = 2, CV_RESID = 3 };
 
 // dynamic shared memory: the element tile (CV_BLOCK Np doubles), then (CUB)
-// the tile of the cubature volume term computed by k_cv_cubvol.
+// Drq, Dsq, Lq (3 Ncub Np) and two buffers of the block's G table for
+// CV_GQ cubature points (2 x 4 x CV_GQ x CV_BLOCK), filled by cp.async while
+// the previous points (or the face terms) are computed.
 // Register budget: only the output row and, for the nodal volume, J grad u
 // are held per thread.  The gradient part of every face slot is applied as a
 // rank-one update Dr^T e_n (rx bx + ry by) + Ds^T e_n (sx bx + sy by), the
 // nodal volume node by node, and the element's u stays in the shared tile.
 template <int N, bool CUB, int MODE>
-__global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 4) k_cv_gather(CvArgs a, const double* __restrict__ u,
+__global__ void __launch_bounds__(CV_BLOCK, CUB ? (N >= 5 ? 2 : 3) : 4) k_cv_gather(CvArgs a, const double* __restrict__ u,
                                                                     const double* __restrict__ b,
                                                                     double* __restrict__ y, double alpha,
                                                                     double shift) {
@@ -200,7 +214,26 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 4) k_cv_gather(CvArgs a, c
   double* s_m = s_dyn + CV_BLOCK * Np;
   const int k0 = blockIdx.x * CV_BLOCK, nk = min(CV_BLOCK, a.K - k0);
   stage_tile<Np>(u, k0, nk, s_u);
-  if (CUB) stage_tile<Np>(a.vol, k0, nk, s_m);
+  double* s_g = s_m + (CUB ? cv_even(3 * a.Ncub * Np) : 0);   // 16-byte aligned for cp.async
+  const int nch = CUB ? (a.Ncub + CV_GQ - 1) / CV_GQ : 0;
+  // the block's G rows of points [ch CV_GQ, (ch + 1) CV_GQ): 128 consecutive
+  // doubles per (field, point), 16-byte pieces (a.ldc and k0 are multiples
+  // of CV_BLOCK, so every piece is aligned and inside the padded table)
+  auto issue = [&](int ch) {
+    double* dst = s_g + (size_t)(ch & 1) * 4 * CV_GQ * CV_BLOCK;
+    for (int idx = threadIdx.x; idx < 4 * CV_GQ * (CV_BLOCK / 2); idx += CV_BLOCK) {
+      const int row = idx / (CV_BLOCK / 2), piece = idx - row * (CV_BLOCK / 2);
+      const int c = row / CV_GQ, q = ch * CV_GQ + (row - c * CV_GQ);
+      if (q < a.Ncub)
+        cp_async16(dst + (size_t)row * CV_BLOCK + 2 * piece,
+                   a.cG + (size_t)(c * a.Ncub + q) * a.ldc + k0 + 2 * piece);
+    }
+    cp_async_commit();
+  };
+  if (CUB) {
+    for (int i = threadIdx.x; i < 3 * a.Ncub * Np; i += CV_BLOCK) s_m[i] = a.cMat[i];
+    issue(0);
+  }
   __syncthreads();
   const bool active = (int)threadIdx.x < nk;
   const int k = k0 + threadIdx.x;
@@ -281,12 +314,46 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 4) k_cv_gather(CvArgs a, c
           out[i] = fma(alpha * a.gN[(4 * Np + i) * K + k], s, out[i]);
         }
       }
-    } else {
-      // cubature volume and mass: computed by k_cv_cubvol into a.vol
-      const double* ve = s_m + threadIdx.x * Np;
-#pragma unroll
-      for (int i = 0; i < Np; ++i) out[i] += ve[i];
     }
+  }
+  if (CUB) {
+    // cubature volume and mass, CV_GQ points at a time from the staged G
+    const double* Drq = s_m;
+    const double* Dsq = s_m + a.Ncub * Np;
+    const double* Lq = s_m + 2 * a.Ncub * Np;
+    double uv[Np];
+#pragma unroll
+    for (int j = 0; j < Np; ++j) uv[j] = active ? ue[j] : 0.0;
+    for (int ch = 0; ch < nch; ++ch) {
+      if (ch + 1 < nch) issue(ch + 1);
+      else cp_async_commit();                      // an empty group keeps the count uniform
+      cp_async_wait_1();                           // chunk ch has landed (this thread's pieces)
+      __syncthreads();                             // ... and every thread's
+      const double* g = s_g + (size_t)(ch & 1) * 4 * CV_GQ * CV_BLOCK + threadIdx.x;
+      if (active) {
+#pragma unroll 1
+        for (int qq = 0; qq < CV_GQ; ++qq) {
+          const int q = ch * CV_GQ + qq;
+          if (q >= a.Ncub) break;
+          double ur = 0.0, us = 0.0, uq = 0.0;
+#pragma unroll
+          for (int j = 0; j < Np; ++j) {
+            ur = fma(Drq[q * Np + j], uv[j], ur);
+            us = fma(Dsq[q * Np + j], uv[j], us);
+            uq = fma(Lq[q * Np + j], uv[j], uq);
+          }
+          const double Grr = g[(0 * CV_GQ + qq) * CV_BLOCK], Grs = g[(1 * CV_GQ + qq) * CV_BLOCK];
+          const double Gss = g[(2 * CV_GQ + qq) * CV_BLOCK], wJ = g[(3 * CV_GQ + qq) * CV_BLOCK];
+          const double vr = fma(Grr, ur, Grs * us), vs = fma(Grs, ur, Gss * us), vm = alpha * wJ * uq;
+#pragma unroll
+          for (int i = 0; i < Np; ++i)
+            out[i] = fma(Drq[q * Np + i], vr, fma(Dsq[q * Np + i], vs, fma(Lq[q * Np + i], vm, out[i])));
+        }
+      }
+      __syncthreads();                             // the buffer is refilled two chunks later
+    }
+  }
+  if (active) {
     if (shift != 0.0) {
 #pragma unroll
       for (int i = 0; i < Np; ++i) out[i] = fma(shift, ue[i], out[i]);
@@ -345,75 +412,6 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? 3 : 4) k_cv_gather(CvArgs a, c
   }
 }
 
-// ------------------------------------------------------- cubature volume
-// vol = sum_q Drq^T (G_rr ur + G_rs us) + Dsq^T (G_rs ur + G_ss us)
-//       + alpha Lq^T (wJ Lq u)            (sipg.py:190-201; cubature.py:243-254)
-// CV_TPE threads per element split the cubature points (point q to thread
-// q mod CV_TPE) and add their partial rows with warp shuffles, so the G
-// table streams through many more warps than one thread per element allows.
-constexpr int CV_TPE = 4;
-template <int N>
-__global__ void __launch_bounds__(CV_BLOCK, 2) k_cv_cubvol(CvArgs a, const double* __restrict__ u, double alpha) {
-  constexpr int Np = CvDim<N>::Np, EPB = CV_BLOCK / CV_TPE;
-  if (a.ctl && a.gate && a.ctl->cont == 0) return;
-  extern __shared__ __align__(16) double s_dyn[];
-  double* s_u = s_dyn;                 // EPB Np
-  double* s_m = s_dyn + EPB * Np;      // Drq, Dsq, Lq
-  const int k0 = blockIdx.x * EPB, nk = min(EPB, a.K - k0);
-  stage_tile<Np>(u, k0, nk, s_u);
-  for (int i = threadIdx.x; i < 3 * a.Ncub * Np; i += CV_BLOCK) s_m[i] = a.cMat[i];
-  __syncthreads();
-  const int e = threadIdx.x / CV_TPE, t = threadIdx.x % CV_TPE;
-  const bool active = e < nk;
-  const int k = k0 + (active ? e : 0);
-  const size_t K = (size_t)a.K;
-  const double* Drq = s_m;
-  const double* Dsq = s_m + a.Ncub * Np;
-  const double* Lq = s_m + 2 * a.Ncub * Np;
-  double uv[Np], out[Np];
-#pragma unroll
-  for (int j = 0; j < Np; ++j) {
-    uv[j] = active ? s_u[e * Np + j] : 0.0;
-    out[j] = 0.0;
-  }
-#pragma unroll 1
-  for (int q = t; q < a.Ncub; q += CV_TPE) {
-    double ur = 0.0, us = 0.0, uq = 0.0;
-#pragma unroll
-    for (int j = 0; j < Np; ++j) {
-      ur = fma(Drq[q * Np + j], uv[j], ur);
-      us = fma(Dsq[q * Np + j], uv[j], us);
-      uq = fma(Lq[q * Np + j], uv[j], uq);
-    }
-    double Grr = 0.0, Grs = 0.0, Gss = 0.0, wJ = 0.0;
-    if (active) {
-      Grr = a.cG[(size_t)(0 * a.Ncub + q) * K + k];
-      Grs = a.cG[(size_t)(1 * a.Ncub + q) * K + k];
-      Gss = a.cG[(size_t)(2 * a.Ncub + q) * K + k];
-      wJ = a.cG[(size_t)(3 * a.Ncub + q) * K + k];
-    }
-    const double vr = fma(Grr, ur, Grs * us), vs = fma(Grs, ur, Gss * us), vm = alpha * wJ * uq;
-#pragma unroll
-    for (int i = 0; i < Np; ++i)
-      out[i] = fma(Drq[q * Np + i], vr, fma(Dsq[q * Np + i], vs, fma(Lq[q * Np + i], vm, out[i])));
-  }
-  // the CV_TPE threads of an element are adjacent lanes of one warp
-#pragma unroll
-  for (int i = 0; i < Np; ++i) {
-#pragma unroll
-    for (int o = 1; o < CV_TPE; o <<= 1) out[i] += __shfl_xor_sync(0xffffffffu, out[i], o);
-  }
-  __syncthreads();
-  if (active) {
-#pragma unroll
-    for (int i = 0; i < Np; ++i)
-      if (i % CV_TPE == t) s_u[e * Np + i] = out[i];
-  }
-  __syncthreads();
-  const size_t off = (size_t)k0 * Np;
-  for (int i = threadIdx.x; i < nk * Np; i += CV_BLOCK) a.vol[off + i] = s_u[i];
-}
-
 // ------------------------------------------------------------- mass, loads
 // y = M_quad f: J (M f) at the nodes (nodal) or Lq^T (w J (Lq f)) (cubature,
 // src/ddg/dg2d/cubature.py:243-254)
@@ -445,7 +443,7 @@ __global__ void __launch_bounds__(CV_BLOCK) k_cv_mass(CvArgs a, const double* __
         double fq = 0.0;
 #pragma unroll
         for (int j = 0; j < Np; ++j) fq = fma(s_m[q * Np + j], fv[j], fq);
-        fq *= a.cG[(size_t)(3 * a.Ncub + q) * K + k];
+        fq *= a.cG[(size_t)(3 * a.Ncub + q) * a.ldc + k];
 #pragma unroll
         for (int i = 0; i < Np; ++i) out[i] = fma(s_m[q * Np + i], fq, out[i]);
       }
@@ -614,14 +612,8 @@ template <int N, bool CUB, int MODE>
 cudaError_t gather_n(const CvArgs& a, const double* u, const double* b, double* y, double alpha, double shift,
                      cudaStream_t s) {
   constexpr int Np = CvDim<N>::Np;
-  const size_t smem = (size_t)(CV_BLOCK * Np * (CUB ? 2 : 1)) * sizeof(double);
-  if (CUB) {
-    constexpr int EPB = CV_BLOCK / CV_TPE;
-    const size_t sv = (size_t)(EPB * Np + 3 * a.Ncub * Np) * sizeof(double);
-    k_cv_cubvol<N><<<(a.K + EPB - 1) / EPB, CV_BLOCK, sv, s>>>(a, u, alpha);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
+  const size_t smem =
+      (size_t)(CV_BLOCK * Np + (CUB ? cv_even(3 * a.Ncub * Np) + 2 * 4 * CV_GQ * CV_BLOCK : 0)) * sizeof(double);
   k_cv_gather<N, CUB, MODE><<<(a.K + CV_BLOCK - 1) / CV_BLOCK, CV_BLOCK, smem, s>>>(a, u, b, y, alpha, shift);
   return cudaGetLastError();
 }
@@ -685,7 +677,6 @@ cudaError_t cv_prepare_n() {
   CV_A((k_cv_gather<N, false, CV_SUB>));
   CV_A((k_cv_gather<N, false, CV_PDOT>));
   CV_A((k_cv_gather<N, false, CV_RESID>));
-  CV_A((k_cv_cubvol<N>));
   CV_A((k_cv_mass<N, true>));
   CV_A((k_cv_mass<N, false>));
 #undef CV_A
@@ -730,6 +721,11 @@ cudaError_t cv_upload_ref(int N, const double* Dr, const double* Ds, const doubl
 #define C_(n) cv_upload_n<n>(Dr, Ds, M, m1d)
   CV_DISPATCH(N, C_);
 #undef C_
+}
+
+size_t cv_gather_smem_bytes(int N, int Ncub) {
+  const int Np = (N + 1) * (N + 2) / 2;
+  return (size_t)(cv::CV_BLOCK * Np + cv::cv_even(3 * Ncub * Np) + 2 * 4 * cv::CV_GQ * cv::CV_BLOCK) * sizeof(double);
 }
 
 cudaError_t cv_prepare(int N) {

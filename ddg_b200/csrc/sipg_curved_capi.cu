@@ -57,7 +57,8 @@ struct ddg_curved_op {
   double tau_scale = 0.0;
   double *gN = nullptr, *fN = nullptr, *sJ0 = nullptr, *tauF = nullptr;
   double *cG = nullptr, *cQ = nullptr, *cMat = nullptr;
-  double *tr = nullptr, *dl = nullptr, *zero = nullptr, *vol = nullptr;
+  double *tr = nullptr, *dl = nullptr, *zero = nullptr;
+  int ldc = 0;                      // row stride of cG (K rounded up to 128)
   int *tag = nullptr, *slotP = nullptr, *mapP = nullptr, *colour = nullptr;
   unsigned int* status = nullptr;
   CgCtl* ctl = nullptr;
@@ -91,7 +92,7 @@ CvArgs cv_args(const ddg_curved_op* op, int gate) {
   a.cMat = op->cMat;
   a.tr = op->tr;
   a.dl = op->dl;
-  a.vol = op->vol;
+  a.ldc = op->ldc;
   a.ctl = op->ctl;
   a.partA = op->partA;
   a.partB = op->partB;
@@ -135,7 +136,7 @@ void cv_free(ddg_curved_op* op) {
   }
   op->graphs.clear();
   for (void* ptr : {(void*)op->gN, (void*)op->fN, (void*)op->sJ0, (void*)op->tauF, (void*)op->cG, (void*)op->cQ,
-                    (void*)op->cMat, (void*)op->tr, (void*)op->dl, (void*)op->zero, (void*)op->vol, (void*)op->tag,
+                    (void*)op->cMat, (void*)op->tr, (void*)op->dl, (void*)op->zero, (void*)op->tag,
                     (void*)op->slotP, (void*)op->mapP, (void*)op->colour, (void*)op->status, (void*)op->ctl,
                     (void*)op->partA, (void*)op->partB, (void*)op->blocks, (void*)op->binv, (void*)op->x,
                     (void*)op->r, (void*)op->z, (void*)op->p, (void*)op->Ap, (void*)op->b})
@@ -233,7 +234,7 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
   if (Ncub > 0 && (Nfq < 1 || !d->cw || !d->Drq || !d->Dsq || !d->Lq || !d->cJ || !d->crx || !d->csx || !d->cry ||
                    !d->csy || !d->face_w || !d->face_L1d || !d->face_sJ))
     return fail(DDG_ERR_INVALID, "ddg_curved_create: cubature arrays missing");
-  if ((size_t)(32 * Np + 3 * (size_t)Ncub * Np) * sizeof(double) > (size_t)CV_SMEM_LIMIT)
+  if (Ncub > 0 && cv_gather_smem_bytes(N, Ncub) > (size_t)CV_SMEM_LIMIT)
     return fail(DDG_ERR_UNSUPPORTED, "cubature rule too large for the staged kernels (Ncub = " + std::to_string(Ncub) +
                                          ")");
   for (int p = 0; p < Nfp; ++p)
@@ -304,17 +305,18 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
     }
   std::vector<double> cG, cQ, cMat;
   const int NQ = Nfp * (Nfp + 1) / 2;
+  const int ldc = (K + 127) / 128 * 128;
   if (Ncub > 0) {
-    cG.resize((size_t)4 * Ncub * K);
+    cG.assign((size_t)4 * Ncub * ldc, 0.0);
     for (int q = 0; q < Ncub; ++q)
       for (int k = 0; k < K; ++k) {
         const size_t i = (size_t)q * K + k;
         const double wJ = d->cw[q] * d->cJ[i];
         const double rx = d->crx[i], sx = d->csx[i], ry = d->cry[i], sy = d->csy[i];
-        cG[(size_t)(0 * Ncub + q) * K + k] = wJ * (rx * rx + ry * ry);
-        cG[(size_t)(1 * Ncub + q) * K + k] = wJ * (rx * sx + ry * sy);
-        cG[(size_t)(2 * Ncub + q) * K + k] = wJ * (sx * sx + sy * sy);
-        cG[(size_t)(3 * Ncub + q) * K + k] = wJ;
+        cG[(size_t)(0 * Ncub + q) * ldc + k] = wJ * (rx * rx + ry * ry);
+        cG[(size_t)(1 * Ncub + q) * ldc + k] = wJ * (rx * sx + ry * sy);
+        cG[(size_t)(2 * Ncub + q) * ldc + k] = wJ * (sx * sx + sy * sy);
+        cG[(size_t)(3 * Ncub + q) * ldc + k] = wJ;
       }
     cQ.assign((size_t)3 * NQ * K, 0.0);
     for (int f = 0; f < 3; ++f)
@@ -344,6 +346,7 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
   op->Ncub = Ncub;
   op->Nfq = Nfq;
   op->ncol = ncol;
+  op->ldc = ldc;
   op->tau_scale = d->tau_scale;
   const int nparts = std::max((K + 127) / 128, xr_grid((int64_t)K * Np)) + 32;
   cudaError_t e = cudaSuccess;
@@ -370,7 +373,6 @@ extern "C" int ddg_curved_create(const ddg_curved_desc* d, ddg_curved_op** out) 
     ALLOC(op->cG, cG.size() * 8);
     ALLOC(op->cQ, cQ.size() * 8);
     ALLOC(op->cMat, cMat.size() * 8);
-    ALLOC(op->vol, KN * 8);
   }
   UPLOAD(op->gN, gN);
   UPLOAD(op->fN, fN);

@@ -140,12 +140,12 @@ struct CvArgs {
   const int* tag;      // [3][K] BC tag of (k, f)
   const int* slotP;    // [3Nfp][K] vmapP: element-major index of the outside trace node
   const int* mapP;     // [3Nfp][K] the matching face slot of the neighbour, m' K + k'
-  const double* cG;    // [4][Ncub][K] wJ(rx^2+ry^2), wJ(rx sx+ry sy), wJ(sx^2+sy^2), wJ
+  const double* cG;    // [4][Ncub][ldc] wJ(rx^2+ry^2), wJ(rx sx+ry sy), wJ(sx^2+sy^2), wJ
+  int ldc;             // row stride of cG: K rounded up to a multiple of 128 (zero padded)
   const double* cQ;    // [3][Nfp(Nfp+1)/2][K] packed face rule L1d^T diag(face_w sJ) L1d
   const double* cMat;  // [3][Ncub][Np] Drq, Dsq, Lq
   double* tr;          // [2][3Nfp][K] gradient traces (pass 1)
   double* dl;          // [3][3Nfp][K] face duals (pass 2)
-  double* vol;         // element-major cubature volume (+ mass) term of the gather pass
   CgCtl* ctl;          // CG control block (PDOT, RESID; gating inside CG graphs)
   double* partA;       // per-block partials
   double* partB;
@@ -159,6 +159,8 @@ struct CvArgs {
 cudaError_t launch_cv_pass(int N, int pass, int quad, int mode, const CvArgs& a, const double* u, const double* udir,
                            const double* b, double* y, double alpha, double shift, cudaStream_t s);
 cudaError_t cv_prepare(int N);
+// dynamic shared memory of the cubature gather pass for degree N, Ncub points
+size_t cv_gather_smem_bytes(int N, int Ncub);
 // the curved kernels' copy of the reference-element matrices
 cudaError_t cv_upload_ref(int N, const double* Dr, const double* Ds, const double* M, const double* m1d);
 cudaError_t launch_cv_mass(int N, int quad, const CvArgs& a, const double* f, double* y, cudaStream_t s);
