@@ -13,8 +13,9 @@ The explicit parts of the step -- the Lax-Friedrichs advection term, the
 divergence and gradient, and the consistent pressure-Neumann data -- are
 elementwise float64 numpy on the host, restated from the reference
 (``incompressible_ns.py:100-320``, ``maxwell.py:31-42``); they are not part
-of the SIPG solve path this package accelerates.  Curved-element cubature,
-velocity reconstruction and the penalty post-projection are not supported.
+of the SIPG solve path this package accelerates.  Curved meshes run with or
+without ``cub``; velocity reconstruction and the penalty post-projection are
+not supported.
 """
 
 from __future__ import annotations
@@ -161,9 +162,8 @@ def build_ins_operators(mesh: Mesh2D, *, dt: float, nu: float, g0: float, ins_bc
                         skip_factor: bool = False, cub=None) -> INSOperators:
     """``build_ins_operators`` (``:415-458``).  With ``skip_factor`` (the
     iterative path) nothing dense is built; the device operators are created
-    lazily by the solves and kept resident on the mesh."""
-    if cub is not None:
-        raise ValueError("curved-element cubature (cub=...) is not supported")
+    lazily by the solves and kept resident on the mesh.  ``cub`` (curved
+    meshes) factors the cubature operators, as the reference does."""
     p_bc = pressure_bc_types_from_ins(ins_bc_types)
     v_bc = viscous_bc_types_from_ins(ins_bc_types)
     alpha = g0 / (nu * dt)
@@ -171,8 +171,8 @@ def build_ins_operators(mesh: Mesh2D, *, dt: float, nu: float, g0: float, ins_bc
     if skip_factor:
         pf = vf = None
     else:
-        pf = factor_sipg_2d(mesh, bc_types=p_bc, tau_scale=tau_scale, regularize=p_sing)
-        vf = factor_sipg_helmholtz_2d(mesh, alpha=alpha, nu=nu, bc_types=v_bc, tau_scale=tau_scale)
+        pf = factor_sipg_2d(mesh, bc_types=p_bc, tau_scale=tau_scale, regularize=p_sing, cub=cub)
+        vf = factor_sipg_helmholtz_2d(mesh, alpha=alpha, nu=nu, bc_types=v_bc, tau_scale=tau_scale, cub=cub)
     return INSOperators(pf, vf, p_bc, v_bc, alpha)
 
 
@@ -204,12 +204,12 @@ def ns_step_2d(mesh: Mesh2D, ux_n, uy_n, ux_old, uy_old, Nux_old, Nuy_old, dpdn_
     """One dual-splitting step (``:509-666``): advection and BDF
     extrapolation, pressure Poisson with the extrapolated consistent Neumann
     data, pressure-gradient correction, then one viscous Helmholtz solve per
-    velocity component warm-started from ``ux_n`` / ``uy_n``.  Returns
+    velocity component warm-started from ``ux_n`` / ``uy_n``.  With ``cub``
+    (curved meshes) the three solves use the cubature operator and mass, as
+    ``_pressure_solve`` / ``_viscous_solve`` do (``:669-805``).  Returns
     ``(ux, uy, p, Nux, Nuy, dpdn)``."""
     if penalty_factored is not None or penalty_iterative is not None:
         raise ValueError("the penalty post-projection is not supported")
-    if cub is not None:
-        raise ValueError("curved-element cubature (cub=...) is not supported")
     g0 = bdf.g0
     ux_n, uy_n = np.asarray(ux_n, dtype=np.float64), np.asarray(uy_n, dtype=np.float64)
     nux, nuy = ns_advection_2d(mesh, ux_n, uy_n, ins_bc_types=ins_bc_types, bc_ux=bc_ux, bc_uy=bc_uy,
@@ -224,15 +224,15 @@ def ns_step_2d(mesh: Mesh2D, ux_n, uy_n, ux_old, uy_old, Nux_old, Nuy_old, dpdn_
     dpdn_x = bdf.b0 * dpdn_n + bdf.b1 * np.asarray(dpdn_old)
     p = solve_sipg_poisson_2d(mesh, p_source, bc_types=ops.pressure_bc_types, u_dir=p_dir, q_neu=dpdn_x,
                               tau_scale=tau_scale, A_factored=ops.pressure_factored, iterative=iterative,
-                              preconditioner=pressure_preconditioner)
+                              preconditioner=pressure_preconditioner, cub=cub)
     dpdx, dpdy = grad_2d(mesh, p)
     ux_tt = ux_t - (dt / g0) * dpdx
     uy_tt = uy_t - (dt / g0) * dpdy
     a = ops.alpha
     ux = solve_sipg_helmholtz_2d(mesh, a * ux_tt, alpha=a, nu=nu, bc_types=ops.viscous_bc_types, u_dir=bc_ux,
                                  q_neu=q_ux_neu, tau_scale=tau_scale, A_factored=ops.viscous_factored,
-                                 iterative=iterative, x0=ux_n, preconditioner=viscous_preconditioner)
+                                 iterative=iterative, x0=ux_n, preconditioner=viscous_preconditioner, cub=cub)
     uy = solve_sipg_helmholtz_2d(mesh, a * uy_tt, alpha=a, nu=nu, bc_types=ops.viscous_bc_types, u_dir=bc_uy,
                                  q_neu=q_uy_neu, tau_scale=tau_scale, A_factored=ops.viscous_factored,
-                                 iterative=iterative, x0=uy_n, preconditioner=viscous_preconditioner)
+                                 iterative=iterative, x0=uy_n, preconditioner=viscous_preconditioner, cub=cub)
     return ux, uy, p, nux, nuy, dpdn_n

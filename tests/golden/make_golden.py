@@ -186,6 +186,43 @@ def curved_fixtures(imp) -> dict:
     print(f"curved helmholtz CG {refshim.cg_last_iterations()} its {time.time() - t0:.1f}s", flush=True)
     out["cyl8_N4/helm/u_lu"] = _a(rsipg.solve_sipg_helmholtz_2d(m, rhs, alpha=5.0, nu=1.0, bc_types=bc,
                                                                  tau_scale=0.5, cub=cub))
+    # one dual-splitting step on the cylinder mesh (N = 3) with cubature:
+    # inflow x = 0, outflow x = 2, walls y = 0, 2, the cylinder an obstacle;
+    # direct LU and matrix-free CG
+    rins = imp("ddg.dg2d.incompressible_ns")
+    VX2, VY2, E2 = _a(out["cyl8_N4/VX"]), _a(out["cyl8_N4/VY"]), _a(out["cyl8_N4/EToV"])
+    m3 = rcur.apply_circular_hole_2d(rmesh.build_mesh_2d(VX2, VY2, E2, 3), cx=1.0, cy=1.0, radius=0.25,
+                                     detection_tol=0.1)
+    cub3 = rcub.attach_cubature(m3)
+    K3 = int(m3.K)
+    isb = boundary_faces(m3)
+    xf = _a(m3.x)[_a(m3.Fmask)]                                    # (Nfp, 3, K)
+    yf = _a(m3.y)[_a(m3.Fmask)]
+    on = lambda a, v: np.all(np.abs(a - v) < 1e-7, axis=0).T       # noqa: E731  (K, 3)
+    code = np.where(on(xf, 0.0), rins.BC_INS_INFLOW,
+                    np.where(on(xf, 2.0), rins.BC_INS_OUTFLOW,
+                             np.where(on(yf, 0.0) | on(yf, 2.0), rins.BC_INS_WALL, rins.BC_INS_OBSTACLE)))
+    ins_bc = np.where(isb, code, rins.BC_INS_INTERIOR).astype(np.int32)
+    x3, y3 = _a(m3.x), _a(m3.y)
+    ux0 = 0.2 * y3 * (2.0 - y3)
+    uy0 = 0.05 * np.sin(np.pi * x3) * y3 * (2.0 - y3)
+    bcux = np.where(np.abs(x3) < 1e-9, y3 * (2.0 - y3), 0.0)
+    zero = np.zeros_like(x3)
+    dt, nu = 0.01, 0.05
+    nxo, nyo = rins.ns_advection_2d(m3, ux0, uy0, ins_bc_types=ins_bc, bc_ux=bcux, bc_uy=zero)
+    dpdn0 = np.zeros((3 * int(m3.Nfp), K3))
+    args = (m3, ux0, uy0, ux0, uy0, nxo, nyo, dpdn0)
+    kw = dict(dt=dt, nu=nu, bdf=rins.BDF1, ins_bc_types=ins_bc, bc_ux=bcux, bc_uy=zero, cub=cub3)
+    ops = rins.build_ins_operators(m3, dt=dt, nu=nu, g0=1.0, ins_bc_types=ins_bc, cub=cub3)
+    res_lu = rins.ns_step_2d(*args, ops=ops, **kw)
+    ops_mf = rins.build_ins_operators(m3, dt=dt, nu=nu, g0=1.0, ins_bc_types=ins_bc, skip_factor=True, cub=cub3)
+    res_cg = rins.ns_step_2d(*args, ops=ops_mf, iterative=IC(tol=1e-12, maxiter=20000), **kw)
+    out["ins_cyl_N3/ins_bc"] = ins_bc
+    out["ins_cyl_N3/ux0"], out["ins_cyl_N3/uy0"], out["ins_cyl_N3/bc_ux"] = ux0, uy0, bcux
+    out["ins_cyl_N3/Nux_old"], out["ins_cyl_N3/Nuy_old"] = _a(nxo), _a(nyo)
+    for tag, res in (("lu", res_lu), ("cg", res_cg)):
+        for name, v in zip(("ux", "uy", "p", "Nux", "Nuy", "dpdn"), res):
+            out[f"ins_cyl_N3/{tag}/{name}"] = _a(v)
     print(f"curved done {time.time() - t0:.1f}s", flush=True)
     return out
 

@@ -214,3 +214,19 @@ def test_curved_entry_points_exported():
               "ddg_curved_pc_apply", "ddg_curved_pc_blocks", "ddg_curved_cg"):
         assert n in names
         assert hasattr(_lib.lib(), n)
+
+
+def test_ins_explicit_terms_on_curved_mesh_match_reference():
+    """The host-side explicit terms of the dual-splitting step (advection
+    with the Lax-Friedrichs flux) on the bent cylinder mesh, against the
+    reference's own ns_advection_2d there."""
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import incompressible_ns as pins
+    from ddg_b200.dg2d import mesh as pm
+    g = _g()
+    m = pcur.apply_circular_hole_2d(pm.build_mesh_2d(g["cyl8_N4/VX"], g["cyl8_N4/VY"], g["cyl8_N4/EToV"], 3),
+                                    cx=1.0, cy=1.0, radius=0.25, detection_tol=0.1)
+    k = "ins_cyl_N3/"
+    nx, ny = pins.ns_advection_2d(m, g[k + "ux0"], g[k + "uy0"], ins_bc_types=g[k + "ins_bc"], bc_ux=g[k + "bc_ux"],
+                                  bc_uy=np.zeros_like(m.x))
+    assert _rel(nx, g[k + "Nux_old"]) < 1e-11 and _rel(ny, g[k + "Nuy_old"]) < 1e-11

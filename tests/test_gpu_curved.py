@@ -262,3 +262,32 @@ def test_curved_cg_zero_rhs_and_errors():
     with pytest.raises(ValueError):
         sipg.solve_sipg_poisson_2d(p, np.ones((p.Np, p.K)), bc_types=bc, cub=pc_,
                                    iterative=sipg.IterativeConfig(precision="mixed"))
+
+
+@pytest.mark.parametrize("path", ["lu", "cg"])
+def test_curved_ins_step_with_cubature_matches_reference(path):
+    """One dual-splitting step (BDF1) of flow past the bent cylinder with
+    cub=attach_cubature(mesh): pressure Poisson (outflow Dirichlet) and the
+    two viscous Helmholtz solves on the cubature operator, by LU and by the
+    device CG, against the reference's own ns_step_2d with cub."""
+    from ddg_b200.dg2d import cubature as pcub
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import incompressible_ns as pins
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg
+    g = _g()
+    m = pcur.apply_circular_hole_2d(pm.build_mesh_2d(g["cyl8_N4/VX"], g["cyl8_N4/VY"], g["cyl8_N4/EToV"], 3),
+                                    cx=1.0, cy=1.0, radius=0.25, detection_tol=0.1)
+    cub = pcub.attach_cubature(m)
+    k = "ins_cyl_N3/"
+    ins_bc, zero = g[k + "ins_bc"], np.zeros_like(m.x)
+    dpdn0 = np.zeros((3 * m.Nfp, m.K))
+    ops = pins.build_ins_operators(m, dt=0.01, nu=0.05, g0=1.0, ins_bc_types=ins_bc, skip_factor=(path == "cg"),
+                                   cub=cub)
+    it = sipg.IterativeConfig(tol=1e-12, maxiter=20000) if path == "cg" else None
+    res = pins.ns_step_2d(m, g[k + "ux0"], g[k + "uy0"], g[k + "ux0"], g[k + "uy0"], g[k + "Nux_old"],
+                          g[k + "Nuy_old"], dpdn0, dt=0.01, nu=0.05, bdf=pins.BDF1, ops=ops, ins_bc_types=ins_bc,
+                          bc_ux=g[k + "bc_ux"], bc_uy=zero, iterative=it, cub=cub)
+    tol = 1e-9 if path == "lu" else 1e-8
+    for name, v in zip(("ux", "uy", "p"), res[:3]):
+        assert _rel(v, g[f"{k}{path}/{name}"]) < tol, (path, name)
