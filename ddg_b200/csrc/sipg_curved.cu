@@ -231,7 +231,14 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? (N >= 5 ? 2 : 3) : 4) k_cv_gat
     cp_async_commit();
   };
   if (CUB) {
-    for (int i = threadIdx.x; i < 3 * a.Ncub * Np; i += CV_BLOCK) s_m[i] = a.cMat[i];
+    // (Drq, Dsq) interleaved as 16-byte pairs, then Lq: one 128-bit and one
+    // 64-bit shared load per basis function and cubature point
+    const int nq = a.Ncub * Np;
+    for (int i = threadIdx.x; i < nq; i += CV_BLOCK) {
+      s_m[2 * i] = a.cMat[i];
+      s_m[2 * i + 1] = a.cMat[nq + i];
+      s_m[2 * nq + i] = a.cMat[2 * nq + i];
+    }
     issue(0);
   }
   __syncthreads();
@@ -318,8 +325,7 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? (N >= 5 ? 2 : 3) : 4) k_cv_gat
   }
   if (CUB) {
     // cubature volume and mass, CV_GQ points at a time from the staged G
-    const double* Drq = s_m;
-    const double* Dsq = s_m + a.Ncub * Np;
+    const double2* DD = reinterpret_cast<const double2*>(s_m);
     const double* Lq = s_m + 2 * a.Ncub * Np;
     double uv[Np];
 #pragma unroll
@@ -338,16 +344,19 @@ __global__ void __launch_bounds__(CV_BLOCK, CUB ? (N >= 5 ? 2 : 3) : 4) k_cv_gat
           double ur = 0.0, us = 0.0, uq = 0.0;
 #pragma unroll
           for (int j = 0; j < Np; ++j) {
-            ur = fma(Drq[q * Np + j], uv[j], ur);
-            us = fma(Dsq[q * Np + j], uv[j], us);
+            const double2 d = DD[q * Np + j];
+            ur = fma(d.x, uv[j], ur);
+            us = fma(d.y, uv[j], us);
             uq = fma(Lq[q * Np + j], uv[j], uq);
           }
           const double Grr = g[(0 * CV_GQ + qq) * CV_BLOCK], Grs = g[(1 * CV_GQ + qq) * CV_BLOCK];
           const double Gss = g[(2 * CV_GQ + qq) * CV_BLOCK], wJ = g[(3 * CV_GQ + qq) * CV_BLOCK];
           const double vr = fma(Grr, ur, Grs * us), vs = fma(Grs, ur, Gss * us), vm = alpha * wJ * uq;
 #pragma unroll
-          for (int i = 0; i < Np; ++i)
-            out[i] = fma(Drq[q * Np + i], vr, fma(Dsq[q * Np + i], vs, fma(Lq[q * Np + i], vm, out[i])));
+          for (int i = 0; i < Np; ++i) {
+            const double2 d = DD[q * Np + i];
+            out[i] = fma(d.x, vr, fma(d.y, vs, fma(Lq[q * Np + i], vm, out[i])));
+          }
         }
       }
       __syncthreads();                             // the buffer is refilled two chunks later
