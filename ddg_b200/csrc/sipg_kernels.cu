@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(ApplyArgs<T> a) {
       if (NT > 1) bulk_load(s_tile[NT - 1], a.in1 + off, bytes, &s_bar);
       s_ok = mbar_wait_bounded(&s_bar, 0, &a.ctl_status[0]) ? 1 : 0;
     }
-    __syncthreads();           // one waiter; the whole block sees its verdict
+    __syncthreads();           // one waiter; the whole block sees its outcome
     if (!s_ok) return;         // uniform exit: no thread is left at a barrier
   } else {
     for (int i = tid; i < nk * Np; i += BLOCK) {
