@@ -110,6 +110,11 @@ def curved_fixtures(imp) -> dict:
     base2 = rmesh.build_mesh_2d(VX2, VY2, E2, 4)
     cyl = rcur.apply_circular_hole_2d(base2, cx=1.0, cy=1.0, radius=0.25, detection_tol=0.1)
     meshes = {"annulus8_N3": (ann, (VX, VY, E)), "cyl8_N4": (cyl, (VX2, VY2, E2))}
+    # the other degrees on the same annulus
+    for Nx in (1, 2, 5):
+        mx = rcur.apply_circular_hole_2d(rmesh.build_mesh_2d(VX, VY, E, Nx), cx=0.0, cy=0.0, radius=0.5,
+                                         detection_tol=0.5)
+        meshes[f"annulus8_N{Nx}"] = (mx, (VX, VY, E))
     cubs = {}
     for name, (m, (vx, vy, ee)) in meshes.items():
         out[f"{name}/VX"], out[f"{name}/VY"], out[f"{name}/EToV"] = _a(vx), _a(vy), _a(ee)

@@ -24,7 +24,7 @@ from oracle import mesh as om
 from oracle import sipg as osp
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ("annulus8_N3", "cyl8_N4")
+NAMES = ("annulus8_N1", "annulus8_N2", "annulus8_N3", "annulus8_N5", "cyl8_N4")
 
 
 def _g():
@@ -87,7 +87,8 @@ def test_product_curved_mesh_and_cubature_match_reference(name):
     g = _g()
     base = pm.build_mesh_2d(g[f"{name}/VX"], g[f"{name}/VY"], g[f"{name}/EToV"], int(g[f"{name}/N"]))
     m = _bend(name, base, pcur)
-    assert base.is_affine and not m.is_affine
+    # degree 1: bending moves only vertices, so the elements stay affine
+    assert base.is_affine and m.is_affine == (m.N == 1)
     assert m._ops is not base._ops
     for f in ("x", "y", "rx", "sx", "ry", "sy", "J", "nx", "ny", "sJ", "Fscale"):
         assert _rel(getattr(m, f), g[f"{name}/mesh/{f}"]) < 2e-12, f
@@ -230,3 +231,28 @@ def test_ins_explicit_terms_on_curved_mesh_match_reference():
     nx, ny = pins.ns_advection_2d(m, g[k + "ux0"], g[k + "uy0"], ins_bc_types=g[k + "ins_bc"], bc_ux=g[k + "bc_ux"],
                                   bc_uy=np.zeros_like(m.x))
     assert _rel(nx, g[k + "Nux_old"]) < 1e-11 and _rel(ny, g[k + "Nuy_old"]) < 1e-11
+
+
+def _annulus24(N=3, curved=True):
+    """The reference test's annulus (test/test_curved_boundary_2d.py:43-59):
+    [-2, 2]^2 with the square hole [-0.5, 0.5]^2, 24 x 24 cells, the inner
+    boundary bent onto the circle of radius 0.5 (detection_tol 0.5)."""
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import mesh as pm
+    VX, VY, E = pm.rectangle_with_square_hole_mesh_2d(-2.0, 2.0, -2.0, 2.0, 24, 24, -0.5, 0.5, -0.5, 0.5)
+    m = pm.build_mesh_2d(VX, VY, E, N)
+    return pcur.apply_circular_hole_2d(m, cx=0.0, cy=0.0, radius=0.5, detection_tol=0.5) if curved else m
+
+
+def test_reference_known_answers_curved_mesh():
+    """The reference's own curved-boundary tests, on the product's builders:
+    the projection moves nodes (max |dx| > 1e-3) and puts every inner
+    boundary node on the circle (radius 0.5 to 1e-10); the mesh stays valid
+    (min J > 0) (test_curved_boundary_2d.py:62-95)."""
+    aff, cur = _annulus24(curved=False), _annulus24()
+    assert np.max(np.abs(cur.x - aff.x)) > 1e-3
+    xb = cur.x.T.reshape(-1)[cur.vmapB]
+    yb = cur.y.T.reshape(-1)[cur.vmapB]
+    rb = np.sqrt(xb ** 2 + yb ** 2)
+    assert np.allclose(rb[rb < 1.0], 0.5, atol=1e-10)
+    assert cur.J.min() > 0.0

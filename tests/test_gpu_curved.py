@@ -14,7 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ("annulus8_N3", "cyl8_N4")
+NAMES = ("annulus8_N1", "annulus8_N2", "annulus8_N3", "annulus8_N5", "cyl8_N4")
 RTOL = 2e-12          # curved operator vs the reference (the product's curved geometry differs by <= 7e-13)
 
 
@@ -291,3 +291,23 @@ def test_curved_ins_step_with_cubature_matches_reference(path):
     tol = 1e-9 if path == "lu" else 1e-8
     for name, v in zip(("ux", "uy", "p"), res[:3]):
         assert _rel(v, g[f"{k}{path}/{name}"]) < tol, (path, name)
+
+
+def test_reference_curved_poisson_known_answer():
+    """The reference's test_curved_poisson_solve_well_behaved at its own size
+    (24 x 24 annulus, N = 3, all-Dirichlet, u = sin(pi x / 4) sin(pi y / 4),
+    direct LU of the nodal-rule operator): relative L2 error < 2e-2 --
+    and with the cubature rule too."""
+    from ddg_b200.dg2d import cubature as pcub
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import mesh as pm
+    from ddg_b200.dg2d import sipg
+    VX, VY, E = pm.rectangle_with_square_hole_mesh_2d(-2.0, 2.0, -2.0, 2.0, 24, 24, -0.5, 0.5, -0.5, 0.5)
+    m = pcur.apply_circular_hole_2d(pm.build_mesh_2d(VX, VY, E, 3), cx=0.0, cy=0.0, radius=0.5, detection_tol=0.5)
+    ue = np.sin(np.pi * m.x / 4) * np.sin(np.pi * m.y / 4)
+    src = 2 * (np.pi / 4) ** 2 * ue
+    bc = np.where(m.EToE == np.arange(m.K)[:, None], 1, 0).astype(np.int32)
+    for cub in (None, pcub.attach_cubature(m)):
+        u = sipg.solve_sipg_poisson_2d(m, src, bc_types=bc, u_dir=ue, cub=cub)
+        err = np.sqrt(np.sum(m.J * (u - ue) ** 2) / np.sum(m.J * ue ** 2))
+        assert err < 2e-2, (cub is not None, err)

@@ -20,7 +20,7 @@ def _port():
     return p
 
 
-@pytest.mark.parametrize("case", ["helmholtz_bj", "poisson_neumann"])
+@pytest.mark.parametrize("case", ["helmholtz_bj", "poisson_neumann", "curved_cub"])
 def test_sharded_single_rank_matches_single_gpu_solve(case):
     import torch.distributed as dist
     from ddg_b200.dg2d import mesh as pm
@@ -38,6 +38,22 @@ def test_sharded_single_rank_matches_single_gpu_solve(case):
             u, info = sh.solve(f, alpha=3.0, tol=1e-10, maxiter=3000)
             pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=3.0, nu=1.0, bc_types=bc, tau_scale=0.5)
             ref, rinfo = ps.solve_sipg_helmholtz_2d(m, f, alpha=3.0, nu=1.0, bc_types=bc, tau_scale=0.5,
+                                                    preconditioner=pc, return_info=True,
+                                                    iterative=ps.IterativeConfig(tol=1e-10, maxiter=3000))
+        elif case == "curved_cub":
+            from ddg_b200.dg2d import cubature as pcub
+            from ddg_b200.dg2d import curved as pcur
+            VX, VY, E = pm.rectangle_with_square_hole_mesh_2d(-2.0, 2.0, -2.0, 2.0, 16, 16, -0.5, 0.5, -0.5, 0.5)
+            m = pcur.apply_circular_hole_2d(pm.build_mesh_2d(VX, VY, E, 3), cx=0.0, cy=0.0, radius=0.5,
+                                            detection_tol=0.5)
+            cub = pcub.attach_cubature(m)
+            bc = np.where(m.EToE == np.arange(m.K)[:, None], 1, 0).astype(np.int32)
+            f = np.cos(m.x) * np.sin(0.7 * m.y) + 0.1
+            sh = ShardedSipg(m, bc, tau_scale=0.5, cub=cub)
+            u, info = sh.solve(f, alpha=2.0, tol=1e-10, maxiter=3000)
+            pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=2.0, nu=1.0, bc_types=bc, tau_scale=0.5,
+                                                               cub=cub)
+            ref, rinfo = ps.solve_sipg_helmholtz_2d(m, f, alpha=2.0, nu=1.0, bc_types=bc, tau_scale=0.5, cub=cub,
                                                     preconditioner=pc, return_info=True,
                                                     iterative=ps.IterativeConfig(tol=1e-10, maxiter=3000))
         else:

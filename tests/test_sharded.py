@@ -53,10 +53,10 @@ class OracleLocalOps:
     """A rank's local operator and vector kernels computed by the oracle on
     the CPU (test stand-in for the device local operator)."""
 
-    def __init__(self, lm, lbc, tau):
+    def __init__(self, lm, lbc, tau, cub=None):
         import torch
         self.torch = torch
-        self.lm, self.bc, self.tau = lm, lbc, tau
+        self.lm, self.bc, self.tau, self.cub = lm, lbc, tau, cub
         self.n = lm.K * lm.Np
         self.device = None
 
@@ -73,19 +73,19 @@ class OracleLocalOps:
 
     def apply(self, v, alpha):
         U = self._field(v)
-        Y = osp.apply(self.lm, U, bc_types=self.bc, tau_scale=self.tau)
+        Y = osp.apply(self.lm, U, bc_types=self.bc, tau_scale=self.tau, cub=self.cub)
         if alpha != 0.0:
-            Y = Y + alpha * osp.mass_apply(self.lm, U)
+            Y = Y + alpha * osp.mass_apply(self.lm, U, self.cub)
         return self.torch.tensor(Y.T.reshape(-1).copy())
 
     def rhs(self, f, u_dir, q_neu):
         fld = lambda v: None if v is None else self._field(v)  # noqa: E731
         q = None if q_neu is None else q_neu.numpy().reshape(self.lm.K, -1).T
-        return self.torch.tensor(osp._rhs(self.lm, fld(f), self.bc, fld(u_dir), q, self.tau).copy())
+        return self.torch.tensor(osp._rhs(self.lm, fld(f), self.bc, fld(u_dir), q, self.tau, self.cub).copy())
 
     def pc_build(self, alpha):
         B = osp.extract_block_diag_matfree(osp.flat_op(self.lm, bc_types=self.bc, tau_scale=self.tau,
-                                                       alpha=alpha), self.lm)
+                                                       alpha=alpha, cub=self.cub), self.lm)
         self.Binv = np.linalg.inv(B)
 
     def pc_apply(self, r):
@@ -113,11 +113,11 @@ def _worker(rank, world, port, name, q):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
         case = CASES[name]
-        m = _mesh()
+        m, cub = case.get("mesh", lambda: (_mesh(), None))()
         kw = case["kw"]
         bc = case["bc"](m)
         tau = kw["tau"]
-        sh = ShardedSipg(m, bc, tau_scale=tau, local_ops=OracleLocalOps)
+        sh = ShardedSipg(m, bc, tau_scale=tau, local_ops=OracleLocalOps, cub=cub)
         u, info = sh.solve(case["src"](m), alpha=kw["alpha"], u_dir=case.get("udir", lambda m: None)(m),
                            tol=kw["tol"], maxiter=2000, preconditioner=kw["pc"])
         if rank == 0:
@@ -126,7 +126,20 @@ def _worker(rank, world, port, name, q):
         dist.destroy_process_group()
 
 
+def _curved_mesh():
+    """A bent annulus (degree 2) with its cubature: the curved branch."""
+    from ddg_b200.dg2d import cubature as pcub
+    from ddg_b200.dg2d import curved as pcur
+    from ddg_b200.dg2d import mesh as pm
+    VX, VY, E = pm.rectangle_with_square_hole_mesh_2d(-2.0, 2.0, -2.0, 2.0, 16, 16, -0.5, 0.5, -0.5, 0.5)
+    m = pcur.apply_circular_hole_2d(pm.build_mesh_2d(VX, VY, E, 2), cx=0.0, cy=0.0, radius=0.5, detection_tol=0.5)
+    return m, pcub.attach_cubature(m)
+
+
 CASES = {
+    "curved_helmholtz_cub": dict(kw=dict(tau=0.5, alpha=2.0, tol=1e-11, pc="block_jacobi"),
+                                 mesh=_curved_mesh, bc=lambda m: _bc(m, 1),
+                                 src=lambda m: np.cos(m.x) * np.sin(0.7 * m.y) + 0.1),
     "helmholtz_bj": dict(kw=dict(tau=0.5, alpha=3.0, tol=1e-11, pc="block_jacobi"),
                          bc=lambda m: _bc(m, 1),
                          src=lambda m: np.sin(2 * m.x) * np.cos(3 * m.y) + 0.2),
@@ -156,15 +169,19 @@ def test_sharded_cg_matches_single_process(world, name):
         p.join(timeout=120)
         assert p.exitcode == 0
     # the single-process oracle solve of the same system
-    m = _mesh()
+    m, cub = case.get("mesh", lambda: (_mesh(), None))()
     kw = case["kw"]
     bc = case["bc"](m)
     udir = case.get("udir", lambda m: None)(m)
-    M = osp.make_block_jacobi(m, bc_types=bc, tau_scale=kw["tau"], alpha=kw["alpha"]) if kw["pc"] else None
+    M = None
+    if kw["pc"]:
+        B = osp.extract_block_diag_matfree(osp.flat_op(m, bc_types=bc, tau_scale=kw["tau"], alpha=kw["alpha"],
+                                                       cub=cub), m)
+        M = osp.block_jacobi_from_blocks(B)
     cfg = osp.IterativeConfig(tol=kw["tol"], maxiter=2000)
     if kw["alpha"] > 0:
         ref, rits = osp.solve_helmholtz(m, case["src"](m), alpha=kw["alpha"], bc_types=bc, tau_scale=kw["tau"],
-                                        iterative=cfg, preconditioner=M, return_info=True)
+                                        iterative=cfg, preconditioner=M, return_info=True, cub=cub)
     else:
         ref, rits = osp.solve_poisson(m, case["src"](m), bc_types=bc, u_dir=udir, tau_scale=kw["tau"],
                                       iterative=cfg, preconditioner=M, return_info=True)
