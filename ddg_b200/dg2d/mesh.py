@@ -180,10 +180,14 @@ class Mesh2D:
 
     @property
     def is_affine(self) -> bool:
-        """True when every element is a straight-sided triangle: the
-        geometric factors are constant over each element (to 1e-10 of their
-        magnitude) and so are the normals and sJ of each face.  Curved
-        meshes (``curved.project_to_curve_2d``) are not."""
+        """True when the straight-sided (affine) kernels apply: every element
+        is a straight-sided triangle -- the geometric factors are constant
+        over each element (to 1e-10 of their magnitude) and so are the
+        normals and sJ of each face -- and the two sides of every interior
+        face see the same face (equal sJ, opposite normals).  Curved meshes
+        (``curved.project_to_curve_2d``) are not: bent elements, and at
+        degree 1 (where bending moves only vertices) the faces whose two
+        sides no longer meet."""
         if self._affine is None:
             def const(a, rows):
                 a = np.asarray(a)
@@ -194,6 +198,15 @@ class Mesh2D:
             first = np.repeat(np.arange(3) * Nfp, Nfp)
             ok = all(const(a, np.zeros(self.Np, dtype=np.int64)) for a in (self.rx, self.sx, self.ry, self.sy, self.J))
             ok = ok and all(const(a, first) for a in (self.nx, self.ny, self.sJ, self.Fscale))
+            if ok:
+                f0 = np.arange(3) * Nfp
+                nx1, ny1, sJ1 = (np.asarray(a)[f0] for a in (self.nx, self.ny, self.sJ))   # (3, K)
+                kp, fp = np.asarray(self.EToE).T, np.asarray(self.EToF).T
+                inner = kp != np.arange(self.K)[None, :]
+                scale = max(float(np.max(sJ1)), 1e-300)
+                ok = (float(np.max(np.abs(nx1 + nx1[fp, kp])[inner], initial=0.0)) <= 1e-10
+                      and float(np.max(np.abs(ny1 + ny1[fp, kp])[inner], initial=0.0)) <= 1e-10
+                      and float(np.max(np.abs(sJ1 - sJ1[fp, kp])[inner], initial=0.0)) <= 1e-10 * scale)
             object.__setattr__(self, "_affine", bool(ok))
         return self._affine
 
