@@ -460,6 +460,19 @@ def curved_leg(steps, hbm):
                      "roofline": {"bound": "hbm", "achieved": B / t / 1e9, "peak": hbm, "unit": "GB/s",
                                   "frac": B / t / 1e9 / hbm, "algorithmic_bytes": B,
                                   "kernels": "k_cv_trace, k_cv_dual, k_cv_gather (one apply)"}}
+    # end to end through the reference-named function with (Np, K) host
+    # arrays: sipg_apply_2d(mesh, u, cub=cub), both PCIe directions inside
+    u_np = np.random.default_rng(5).standard_normal((m.Np, m.K))
+    for _ in range(2):
+        ps.sipg_apply_2d(m, u_np, bc_types=bc, tau_scale=TAU_SCALE, cub=cub)
+    reps = max(5, steps)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ps.sipg_apply_2d(m, u_np, bc_types=bc, tau_scale=TAU_SCALE, cub=cub)
+    te = (time.perf_counter() - t0) / reps
+    out["e2e"] = {"value": n / te / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": int(u_np.nbytes),
+                  "d2h_bytes_per_step": int(u_np.nbytes), "ms_per_step": te * 1e3,
+                  "note": "sipg_apply_2d(mesh, numpy u, cub=cub): pageable host arrays in and out, host wall clock"}
     f = np.cos(0.3 * m.x) * np.sin(0.2 * m.y) + 0.1
     pc = ps.make_helmholtz_block_jacobi_preconditioner(m, alpha=ALPHA, nu=1.0, bc_types=bc, tau_scale=TAU_SCALE,
                                                        cub=cub)
