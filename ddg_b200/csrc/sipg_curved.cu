@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(CV_BLOCK) k_cv_trace(CvArgs a, const double* _
 
 // ---------------------------------------------------------------- pass 2
 template <int N, bool CUB>
-__global__ void __launch_bounds__(CV_BLOCK, CUB ? 4 : 8) k_cv_dual(CvArgs a, const double* __restrict__ u,
+__global__ void __launch_bounds__(CV_BLOCK, 8) k_cv_dual(CvArgs a, const double* __restrict__ u,
                                                       const double* __restrict__ udir) {
   constexpr int Np = CvDim<N>::Np, Nfp = CvDim<N>::Nfp, Ns = CvDim<N>::Ns, NQ = CvDim<N>::NQ;
   if (a.ctl && a.gate && a.ctl->cont == 0) return;
